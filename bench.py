@@ -1,0 +1,386 @@
+#!/usr/bin/env python3
+"""Benchmark: Coulomb gauge fixing of an SU(3) configuration on B200.
+
+A step is one complete gauge fix of the 32^3x64 synthetic configuration (H scale
+0.5, seed 2) from its unfixed state to e2 <= 1e-15 with omega = 1.95, hits = 2:
+every half-sweep of checkerboard over-relaxation, the fused e2 reduction that
+decides when to stop, the periodic reunitarisation, the final reunitarisation,
+the temporal-link transform and the final observables.
+
+  value  site-updates/s of the headline path (FP64, links resident in HBM; each
+         step first restores the unfixed links from a device copy)
+  e2e    the same through the C ABI from pinned host buffers: raw big-endian
+         file bytes in (byte swap + layout on the GPU), reunitarise, fix, G out
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gfc|reference]
+
+Under torchrun every rank fixes its own replica (weak scaling); the timed
+region is bracketed by a barrier and a device synchronisation and the maximum
+over ranks is reported.  --impl reference times the reference's own CPU code
+(built from source into oracle/_ref) on this host's cores.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gaugefix-coulomb_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "time-to-e2<=1e-15 & site-updates/s: mixed vs FP64 on B200; serve p50/p99"
+BYTES_PER_SITE_UPDATE = {"fp64_full": 2016, "fp32_2row": 672}
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="gfc", choices=["gfc", "reference"])
+    p.add_argument("--ns", type=int, default=32)
+    p.add_argument("--nt", type=int, default=64)
+    p.add_argument("--seed", type=int, default=2)
+    p.add_argument("--scale", type=float, default=0.5)
+    p.add_argument("--tol", type=float, default=1e-15)
+    p.add_argument("--no-extras", action="store_true", help="skip the mixed/exact comparison runs")
+    p.add_argument("--cpu-half-sweeps", type=int, default=8, help="CPU baseline sample per step")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------- ranks --
+class Ranks:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.dist, self.torch = dist, torch
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def reduce(self, x, op):
+        if not self.dist:
+            return x
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=getattr(self.dist.ReduceOp, op))
+        return t.item()
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks --
+class Clocks:
+    """nvidia-smi sampling of SM clock, power and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.f = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                     stderr=subprocess.DEVNULL)
+        time.sleep(0.3)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            cols = [c.strip() for c in line.split(",")]
+            if len(cols) < 9:
+                continue
+            try:
+                sm.append(float(cols[1]))
+                smax = max(smax, float(cols[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, cols[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.remove(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ GPU arm --
+def run_gfc(a, rk):
+    import torch
+
+    import gfc
+
+    ns, nt = a.ns, a.nt
+    V = ns ** 3 * nt
+    half = V // 2
+    U0 = gfc.synth_config(ns, nt, a.seed, a.scale)
+    raw = gfc.PinnedBuffer(V * 4 * 144)
+    raw.view(">f8")[:] = U0
+    del U0
+    gt_host = gfc.PinnedBuffer(V * 144)
+    lat = gfc.Lattice(ns, nt, device=rk.local, mixed=True)
+    lat.upload_links(raw.array, 8, byteswap=True)
+    lat.reunitarize()
+    lat.save_links()
+    params = gfc.default_params(tolerance=a.tol)
+    fast = gfc.options(precision=gfc.PREC_FP64_FAST, stop_rule=gfc.STOP_EVERY)
+    stream = torch.cuda.ExternalStream(lat.stream, device=f"cuda:{rk.local}")
+
+    def fix_resident(opts):
+        lat.restore_links()
+        rc, rep = lat.fix(params, opts)
+        if rc < 0:
+            raise RuntimeError(f"fix did not converge: rc={rc}")
+        return rep
+
+    # ---- device-resident headline: FP64 fast, stop at e2 <= tol
+    for _ in range(max(a.warmup, 3)):
+        fix_resident(fast)
+    rk.barrier()
+    lat.sync()
+    torch.cuda.synchronize()
+    clocks = Clocks(rk.local)
+    clocks.start()
+    l0 = lat.kernel_launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    reps = [fix_resident(fast) for _ in range(a.steps)]
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    rk.barrier()
+    launches = lat.kernel_launches - l0
+    clk = clocks.stop()
+    elapsed = ev0.elapsed_time(ev1) * 1e-3
+    elapsed_max = rk.reduce(elapsed, "MAX")
+    sweeps = [r.sweeps for r in reps]
+    updates = sum(sweeps) * half
+    updates_all = rk.reduce(updates, "SUM")
+    value = updates_all / elapsed_max
+    # dominant kernel: the FP64 half-sweep; its average duration inside the fix
+    # loop (CUDA events on the launching stream, includes the periodic reunit)
+    loop_s = sum(r.seconds_sweeps for r in reps)
+    per_launch = loop_s / sum(sweeps)
+    alg_bytes = half * BYTES_PER_SITE_UPDATE["fp64_full"]
+
+    # ---- end to end through the C ABI with host buffers
+    e2e_t = []
+    for k in range(a.warmup + a.steps):
+        lat.sync()
+        t0 = time.perf_counter()
+        lat.upload_links(raw.array, 8, byteswap=True)
+        lat.reunitarize()
+        rc, rep = lat.fix(params, fast)
+        lat.download_gt(8, False, out=gt_host.view(np.float64))
+        t1 = time.perf_counter()
+        if k >= a.warmup:
+            e2e_t.append((t1 - t0, rep.sweeps))
+    e2e_time = rk.reduce(sum(t for t, _ in e2e_t), "MAX")
+    e2e_updates = rk.reduce(sum(s for _, s in e2e_t) * half, "SUM")
+    lat.restore_links()
+
+    extras = {}
+    if not a.no_extras and rk.world == 1:
+        extras = run_extras(a, lat, params, stream, torch, gfc, half)
+    out = dict(value=value, elapsed=elapsed_max, sweeps=sweeps, per_launch=per_launch, alg_bytes=alg_bytes,
+               launches=launches, clocks=clk, e2e_value=e2e_updates / e2e_time, e2e_time=e2e_time,
+               h2d=V * 4 * 144, d2h=V * 144, extras=extras, final_e2=reps[-1].final_residue,
+               first_below=reps[-1].first_below_tol)
+    lat.close()
+    raw.close()
+    gt_host.close()
+    return out
+
+
+def timed_halfsweeps(lat, stream, torch, n, precision):
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lat.halfsweeps(0, 4, 1.95, 2, precision)
+    ev0.record(stream)
+    lat.halfsweeps(0, n, 1.95, 2, precision)
+    ev1.record(stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1) * 1e-3 / n
+
+
+def run_extras(a, lat, params, stream, torch, gfc, half):
+    """Mixed precision and the exact (reference-arithmetic) path on the same input."""
+    res = {}
+    # exact arithmetic, reference check schedule (the drop-in default)
+    lat.restore_links()
+    t0 = time.perf_counter()
+    rc, rep = lat.fix(params, gfc.options(precision=gfc.PREC_FP64_EXACT, stop_rule=gfc.STOP_REFERENCE))
+    res["fp64_exact_reference_schedule"] = dict(
+        seconds=time.perf_counter() - t0, sweeps=rc, final_e2=rep.final_residue,
+        site_updates_per_s=rep.sweeps * half / rep.seconds_sweeps)
+    # fast FP64, every-sweep stop (the headline path), for the same-run comparison
+    lat.restore_links()
+    ps0, pt0 = lat.plaquette()
+    rc, rep64 = lat.fix(params, gfc.options(precision=gfc.PREC_FP64_FAST, stop_rule=gfc.STOP_EVERY))
+    ps64, pt64 = lat.plaquette()
+    res["fp64_fast"] = dict(seconds=rep64.seconds_total, sweeps=rc, final_e2=rep64.final_residue,
+                            functional=rep64.functional, plaq_drift=max(abs(ps64 - ps0), abs(pt64 - pt0)))
+    # mixed: FP32 two-row bulk to e2 < 1e-9, FP64 refinement
+    mixed = gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY)
+    lat.restore_links()
+    lat.fix(params, mixed)   # warm
+    best = None
+    for _ in range(2):
+        lat.restore_links()
+        rc, rep = lat.fix(params, mixed)
+        if best is None or rep.seconds_total < best[1].seconds_total:
+            best = (rc, rep)
+    rc, rep = best
+    psm, ptm = lat.plaquette()
+    res["mixed"] = dict(seconds=rep.seconds_total, sweeps=rc, sweeps_fp32=rep.sweeps_fp32,
+                        final_e2=rep.final_residue, functional=rep.functional,
+                        functional_vs_fp64=rep.functional - rep64.functional,
+                        plaq_drift=max(abs(psm - ps0), abs(ptm - pt0)))
+    res["mixed_speedup_vs_fp64_fast"] = rep64.seconds_total / rep.seconds_total
+    # isolated kernel timings (no fused reduction, no stopping test)
+    lat.restore_links()
+    res["kernel_fp64_fast_s"] = timed_halfsweeps(lat, stream, torch, 64, gfc.PREC_FP64_FAST)
+    lat.restore_links()
+    res["kernel_fp64_exact_s"] = timed_halfsweeps(lat, stream, torch, 32, gfc.PREC_FP64_EXACT)
+    lat.restore_links()
+    return res
+
+
+# ------------------------------------------------------- CPU reference --
+def ref_harness():
+    has512 = "avx512f" in open("/proc/cpuinfo").read()
+    for name in (["ref_harness"] if has512 else []) + ["ref_harness_v3"]:
+        p = os.path.join(ROOT, "oracle", "_ref", name)
+        if os.path.exists(p):
+            return p
+    return None
+
+
+def cpu_reference(a, steps, warmup, half_sweeps):
+    """The reference's own half-sweep loop (OpenMP over timeslices) on this host."""
+    import gfc
+
+    exe = ref_harness()
+    if exe is None:
+        return None
+    ns, nt = a.ns, a.nt
+    U0 = gfc.synth_config(ns, nt, a.seed, a.scale)
+    with tempfile.TemporaryDirectory() as d:
+        cfg = os.path.join(d, "cfg.be")
+        U0.astype(">f8").tofile(cfg)
+        del U0
+        out = subprocess.run([exe, "bench", cfg, str(ns), str(nt), str(half_sweeps), "0", str(steps),
+                              str(warmup)], capture_output=True, text=True, check=True).stdout
+    rows = [ln.split() for ln in out.splitlines() if ln.startswith("step")]
+    upd = sum(float(r[3]) for r in rows)
+    sec = sum(float(r[5]) for r in rows)
+    threads = int(rows[0][7])
+    return dict(value=upd / sec, seconds=sec, threads=threads, per_step=[float(r[5]) for r in rows],
+                exe=os.path.basename(exe))
+
+
+def main():
+    a = parse_args()
+    rk = Ranks()
+    cfg = {"workload": f"{a.ns}^3x{a.nt} SU(3) Coulomb gauge fix to e2<={a.tol:g}, omega 1.95, hits 2",
+           "lattice": [a.ns, a.nt], "seed": a.seed, "h_scale": a.scale, "tolerance": a.tol,
+           "parallelism": f"replicas x{rk.world}" if rk.world > 1 else "1 GPU",
+           "l2": "inputs larger than L2 (1.2 GB of links per replica)"}
+    if a.impl == "reference":
+        if rk.rank == 0:
+            r = cpu_reference(a, a.steps, a.warmup, a.cpu_half_sweeps)
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built on this machine"}))
+            else:
+                line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": "site-updates/s",
+                        "n_gpus": 0, "steps": a.steps, "warmup": a.warmup,
+                        "ms_per_step": 1e3 * r["seconds"] / a.steps, "higher_is_better": True,
+                        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                        "config": cfg,
+                        "cpu_baseline": {"value": r["value"], "unit": "site-updates/s", "cores": r["threads"],
+                                         "kind": "reference",
+                                         "sample": f"{a.cpu_half_sweeps} half-sweeps of {a.ns}^3x{a.nt} per step "
+                                                   f"({r['exe']}, reference OR loop, OpenMP over t)"},
+                        "e2e": {"value": r["value"], "unit": "site-updates/s", "h2d_bytes_per_step": 0,
+                                "d2h_bytes_per_step": 0}}
+                print(json.dumps(line))
+        rk.close()
+        return
+
+    r = run_gfc(a, rk)
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    peak_gbs = peaks.get("hbm_gbs", 6650.0)
+    achieved = r["alg_bytes"] / r["per_launch"] / 1e9
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": "site-updates/s", "n_gpus": rk.world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1e3 * r["elapsed"] / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+        "time_to_tol_s": r["elapsed"] / a.steps, "half_sweeps_per_fix": r["sweeps"],
+        "first_half_sweep_below_tol": r["first_below"], "final_e2": r["final_e2"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+                     "frac": achieved / peak_gbs, "traffic": None,
+                     "kernel": "k_sweep_fast<S64> (FP64 half-sweep, fused e2)",
+                     "bytes_per_launch": r["alg_bytes"], "seconds_per_launch": r["per_launch"],
+                     "peak_source": "measured" if peaks else "fallback"},
+        "e2e": {"value": r["e2e_value"], "unit": "site-updates/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"]},
+        "gpu_launches": r["launches"],
+        "clocks": r["clocks"],
+        "modes": r["extras"],
+    }
+    if rk.rank == 0 and rk.world == 1:
+        steps = 1
+        c = cpu_reference(a, steps, 0, a.cpu_half_sweeps)
+        if c is not None:
+            line["cpu_baseline"] = {"value": c["value"], "unit": "site-updates/s", "cores": c["threads"],
+                                    "kind": "reference",
+                                    "sample": f"{a.cpu_half_sweeps} half-sweeps of {a.ns}^3x{a.nt} "
+                                              f"({c['exe']}, reference OR loop, OpenMP over t)"}
+    if rk.rank == 0:
+        print(json.dumps(line))
+    rk.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,46 @@
+// gfc_internal.h -- declarations shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gfc_device.cuh"
+
+// bits of the device status word
+#define GFC_STATUS_PROJECT_FAIL 1u   // a projectSU3 met a null row (the reference's -1)
+#define GFC_STATUS_NAN          2u   // a reduction produced NaN
+#define GFC_STATUS_CONVERGED    4u   // a device-side stopping test fired
+
+namespace gfc {
+
+// ---- exact FP64 kernels (gfc_kernels_exact.cu)
+void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
+                        cudaStream_t s);
+void launch_reunitarize(double2 *base, uint32_t stride, uint32_t nblk, unsigned *status, cudaStream_t s);
+void launch_identity(double2 *g, const Lat &l, cudaStream_t s);
+int obs_blocks_per_slice(const Lat &l);
+void launch_obs(const double2 *u, const Lat &l, double *part, double *out, double *slice_out, cudaStream_t s);
+void launch_functional(const double2 *u, const Lat &l, double *part, double *out, cudaStream_t s);
+
+// ---- layout transforms (gfc_kernels_io.cu)
+// Raw file bytes (reference AoS order, elem_bytes 8 or 4, optionally big endian)
+// for timeslices [t0, t0+nts) -> SoA FP64 spatial links u and temporal links ut.
+void launch_load_links(const void *raw, int elem_bytes, int swap, const Lat &l, uint32_t t0, uint32_t nts,
+                       double2 *u, double2 *ut, cudaStream_t s);
+// SoA FP64 G of timeslices [t0, t0+nts) -> AoS (elem_bytes 8 or 4, optional swap)
+void launch_store_gt(const double2 *g, const Lat &l, uint32_t t0, uint32_t nts, int elem_bytes, int swap,
+                     void *raw, cudaStream_t s);
+// AoS raw G -> SoA FP64 (warm start)
+void launch_load_gt(const void *raw, int elem_bytes, int swap, const Lat &l, uint32_t t0, uint32_t nts,
+                    double2 *g, cudaStream_t s);
+// SoA links (spatial u, temporal ut) of timeslices [t0, t0+nts) -> AoS raw
+void launch_store_links(const double2 *u, const double2 *ut, const Lat &l, uint32_t t0, uint32_t nts,
+                        int elem_bytes, int swap, void *raw, cudaStream_t s);
+// ut(x) <- G(x) ut(x) G(x+t)^dagger  (deferred temporal transform)
+void launch_temporal_transform(double2 *ut, const double2 *g, const Lat &l, cudaStream_t s);
+// u_d(x) <- G(x) u0_d(x) G(x+d)^dagger for the spatial links (rebuild from originals)
+void launch_apply_gt_spatial(double2 *u, const double2 *u0, const double2 *g, const Lat &l, cudaStream_t s);
+// plaquette partials: [nt][nbx][2] = (spatial sum, temporal sum) of Re Tr/3
+void launch_plaquette(const double2 *u, const double2 *ut, const Lat &l, double *part, double *out,
+                      cudaStream_t s);
+
+}  // namespace gfc

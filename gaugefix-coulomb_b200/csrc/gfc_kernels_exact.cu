@@ -1,0 +1,327 @@
+// gfc_kernels_exact.cu -- FP64 kernels that round exactly like the reference.
+//
+// k_sweep_exact: one checkerboard half-sweep (gauge_fixing.c:773-787) over the sites
+// of one parity, one thread per site.  Each thread builds w(x) from its 3 forward
+// and 3 backward spatial links (calculate_w, gauge_fixing.c:445-531), computes the
+// over-relaxed update with reference arithmetic (xor_update), and applies it to
+// G(x), the 3 forward links and the 3 backward links (updateLocalUG,
+// gauge_fixing.c:600-651).  With even ns no two sites of one parity share a link,
+// so the parallel half-sweep equals the reference's sequential one bit for bit.
+//
+// Temporal links are not touched here: they never enter w, e2, theta or F, so
+// their transformation is applied once at the end (k_temporal_transform).
+//
+// Memory traffic per site-update: 6 links + G read and written = 14 x 144 B.
+#include "gfc_device.cuh"
+#include "gfc_internal.h"
+
+namespace gfc {
+
+template <bool CB>
+__device__ __forceinline__ void site_update_exact(double2 *__restrict__ u, double2 *__restrict__ g,
+                                                  const Lat &l, int par, const Coord &c, double omega,
+                                                  unsigned hits) {
+    const int op = CB ? (par ^ 1) : 0;
+    const int sp = CB ? par : 0;
+    const uint32_t si = CB ? (c.L >> 1) : c.L;
+    uint32_t ib[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) ib[d] = CB ? (back_L(l, c, d) >> 1) : back_L(l, c, d);
+
+    M3 w;
+#pragma unroll
+    for (int k = 0; k < 9; k++) w.e[k] = cz();
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        M3 f, r;
+        load_m(u + uidx(l, d, sp, 0, si), l.vh, f);
+        load_m(u + uidx(l, d, op, 0, ib[d]), l.vh, r);
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++)
+                w.e[EL(a, b)] = xcadd(w.e[EL(a, b)], xcadd(f.e[EL(a, b)], cconj(r.e[EL(b, a)])));
+    }
+
+    M3 upd;
+    xor_update(w, omega, hits, upd);
+
+    M3 m, t;
+    load_m(g + gidx(l, sp, 0, si), l.vh, m);
+    xprod(upd, m, t);
+    store_m(g + gidx(l, sp, 0, si), l.vh, t);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        load_m(u + uidx(l, d, sp, 0, si), l.vh, m);
+        xprod(upd, m, t);
+        store_m(u + uidx(l, d, sp, 0, si), l.vh, t);
+        load_m(u + uidx(l, d, op, 0, ib[d]), l.vh, m);
+        xprod_dag(m, upd, t);
+        store_m(u + uidx(l, d, op, 0, ib[d]), l.vh, t);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_sweep_exact(double2 *__restrict__ u, double2 *__restrict__ g, Lat l,
+                                                     int par, double omega, unsigned hits) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= l.vh) return;
+    Coord c = coord_cb(l, par, i);
+    site_update_exact<true>(u, g, l, par, c, omega, hits);
+}
+
+// Odd ns: same-parity sites meet across the periodic boundary, so updates inside
+// a timeslice depend on their order.  One thread per timeslice visits the slice in
+// the reference's z, y, x order; distinct timeslices share no spatial link.
+__global__ void k_sweep_exact_serial(double2 *__restrict__ u, double2 *__restrict__ g, Lat l, int sweep,
+                                     double omega, unsigned hits) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint32_t)l.nt) return;
+    for (uint32_t r = 0; r < l.vs; r++) {
+        Coord c = coord_lex(l, t * l.vs + r);
+        int even = !((c.x ^ c.y ^ c.z ^ c.t) & 1u);
+        if (even ^ (sweep & 1)) site_update_exact<false>(u, g, l, 0, c, omega, hits);
+    }
+}
+
+void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
+                        cudaStream_t s) {
+    if (l.cb) {
+        int par = sweep & 1;  // BLACKRED_SWEEP: even sites on even sweeps (gauge_fixing.c:42)
+        unsigned blocks = (l.vh + 127) / 128;
+        k_sweep_exact<<<blocks, 128, 0, s>>>(u, g, l, par, omega, hits);
+    } else {
+        unsigned blocks = (l.nt + 31) / 32;
+        k_sweep_exact_serial<<<blocks, 32, 0, s>>>(u, g, l, sweep, omega, hits);
+    }
+}
+
+// ----------------------------------------------------------- reunitarise --
+// reunitarizeField (fields.c:144-187): projectSU3 on every matrix of nmat
+// SoA matrices laid out as [c][stride] blocks starting at base + k*9*stride.
+__global__ void k_reunitarize(double2 *__restrict__ base, uint32_t stride, uint32_t nblk,
+                              unsigned *__restrict__ status) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t k = blockIdx.y;
+    if (i >= stride || k >= nblk) return;
+    double2 *p = base + (size_t)k * 9 * stride + i;
+    M3 m;
+    load_m(p, stride, m);
+    int st = xproject(m);
+    store_m(p, stride, m);
+    if (st) atomicOr(status, GFC_STATUS_PROJECT_FAIL);
+}
+
+void launch_reunitarize(double2 *base, uint32_t stride, uint32_t nblk, unsigned *status, cudaStream_t s) {
+    dim3 grid((stride + 255) / 256, nblk);
+    k_reunitarize<<<grid, 256, 0, s>>>(base, stride, nblk, status);
+}
+
+__global__ void k_identity(double2 *__restrict__ g, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int c = 0; c < 9; c++) g[(size_t)c * n + i] = make_double2((c % 4) == 0 ? 1.0 : 0.0, 0.0);
+}
+
+// G is npar blocks of [9][vh]; treat it as one [9][npar*vh] run per block
+void launch_identity(double2 *g, const Lat &l, cudaStream_t s) {
+    for (int p = 0; p < l.npar; p++)
+        k_identity<<<(l.vh + 255) / 256, 256, 0, s>>>(g + (size_t)p * 9 * l.vh, l.vh);
+}
+
+// ------------------------------------------------------------- observables --
+// Per site: div A (four_potential.c:70-113) -> e2 density sum_a c_a^2
+// (gauge_fixing.c:428-438) and theta density Re Tr(divA divA^dag)
+// (gauge_fixing.c:374-380); block partials per timeslice.
+__device__ __forceinline__ void calc_A(const M3 &u, M3 &A) {
+    // subtractionHermConjTrless3x3 (SU3_ops.c:322-372) then * (-i/2)
+    M3 d;
+    double2 tr = cz();
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        d.e[EL(a, a)] = make_double2(0.0, xm(2.0, u.e[EL(a, a)].y));
+        tr = xcadd(tr, d.e[EL(a, a)]);
+    }
+    tr = make_double2(xd(tr.x, 3.0), xd(tr.y, 3.0));
+#pragma unroll
+    for (int a = 0; a < 3; a++) d.e[EL(a, a)] = xcsub(d.e[EL(a, a)], tr);
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+            if (a != b) d.e[EL(a, b)] = xcsub(u.e[EL(a, b)], cconj(u.e[EL(b, a)]));
+    const double2 al = make_double2(-0.0, -0.5);
+#pragma unroll
+    for (int k = 0; k < 9; k++) A.e[k] = xcmul(al, d.e[k]);
+}
+
+template <bool CB>
+__device__ __forceinline__ void site_obs(const double2 *__restrict__ u, const Lat &l, int par,
+                                         const Coord &c, double &e2, double &th) {
+    const int op = CB ? (par ^ 1) : 0;
+    const int sp = CB ? par : 0;
+    const uint32_t si = CB ? (c.L >> 1) : c.L;
+    M3 dA;
+#pragma unroll
+    for (int k = 0; k < 9; k++) dA.e[k] = cz();
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        uint32_t Lb = back_L(l, c, d);
+        uint32_t ib = CB ? (Lb >> 1) : Lb;
+        M3 f, r, A1, A2;
+        load_m(u + uidx(l, d, sp, 0, si), l.vh, f);
+        load_m(u + uidx(l, d, op, 0, ib), l.vh, r);
+        calc_A(f, A1);
+        calc_A(r, A2);
+#pragma unroll
+        for (int k = 0; k < 9; k++) dA.e[k] = xcadd(dA.e[k], xcsub(A1.e[k], A2.e[k]));
+    }
+    // decomposeAlgebraSU3 (SU3_ops.c:1055-1107)
+    const double2 *m = dA.e;
+    double cc[8];
+    cc[0] = xa(m[EL(0, 1)].x, m[EL(1, 0)].x);
+    cc[1] = xa(-m[EL(0, 1)].y, m[EL(1, 0)].y);
+    cc[2] = xs(m[EL(0, 0)].x, m[EL(1, 1)].x);
+    cc[3] = xa(m[EL(0, 2)].x, m[EL(2, 0)].x);
+    cc[4] = xa(-m[EL(0, 2)].y, m[EL(2, 0)].y);
+    cc[5] = xa(m[EL(1, 2)].x, m[EL(2, 1)].x);
+    cc[6] = xa(-m[EL(1, 2)].y, m[EL(2, 1)].y);
+    cc[7] = xd(xs(xa(m[EL(0, 0)].x, m[EL(1, 1)].x), xm(2.0, m[EL(2, 2)].x)), __dsqrt_rn(3.0));
+    double s = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; a++) s = xa(s, xm(cc[a], cc[a]));
+    e2 = s;
+    // Re Tr(dA dA^dag) = sum_ab |dA_ab|^2 accumulated as the trace of prod3x3
+    double t = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        double2 sa = cz();
+#pragma unroll
+        for (int k = 0; k < 3; k++) sa = xcadd(sa, xcmul(m[EL(a, k)], cconj(m[EL(a, k)])));
+        t = xa(t, sa.x);
+    }
+    th = t;
+}
+
+// block-level deterministic sum of NQ values; result valid in thread 0
+template <int NQ>
+__device__ __forceinline__ void block_sum(double (&v)[NQ]) {
+    __shared__ double sh[NQ][32];
+#pragma unroll
+    for (int q = 0; q < NQ; q++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NQ; q++) sh[q][wid] = v[q];
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            v[q] = lane < nw ? sh[q][lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+        }
+    }
+    __syncthreads();
+}
+
+// grid (nbx, nt): block bx of slice t sums sites of both parities of slice t
+__global__ void __launch_bounds__(256) k_obs_partials(const double2 *__restrict__ u, Lat l,
+                                                      double *__restrict__ part) {
+    const uint32_t t = blockIdx.y;
+    const uint32_t vsh = l.cb ? l.vs / 2 : l.vs;  // slots of one parity per slice
+    const uint32_t n = vsh * l.npar;
+    double v[2] = {0.0, 0.0};
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int par = (int)(k / vsh);
+        uint32_t i = t * vsh + (k % vsh);
+        double e2, th;
+        if (l.cb) {
+            Coord c = coord_cb(l, par, i);
+            site_obs<true>(u, l, par, c, e2, th);
+        } else {
+            Coord c = coord_lex(l, i);
+            site_obs<false>(u, l, 0, c, e2, th);
+        }
+        v[0] += e2;
+        v[1] += th;
+    }
+    block_sum<2>(v);
+    if (threadIdx.x == 0) {
+        size_t o = ((size_t)t * gridDim.x + blockIdx.x) * 2;
+        part[o] = v[0];
+        part[o + 1] = v[1];
+    }
+}
+
+// F density: Re Tr of the 3 spatial links at a site (calculateF, gauge_fixing.c:289-337)
+__global__ void __launch_bounds__(256) k_functional_partials(const double2 *__restrict__ u, Lat l,
+                                                             double *__restrict__ part) {
+    const uint32_t t = blockIdx.y;
+    const uint32_t vsh = l.cb ? l.vs / 2 : l.vs;
+    const uint32_t n = vsh * l.npar;
+    double v[1] = {0.0};
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int par = (int)(k / vsh);
+        uint32_t i = t * vsh + (k % vsh);
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double2 *p = u + uidx(l, d, par, 0, i);
+            v[0] += (p[0].x + p[(size_t)4 * l.vh].x) + p[(size_t)8 * l.vh].x;
+        }
+    }
+    block_sum<1>(v);
+    if (threadIdx.x == 0) part[(size_t)t * gridDim.x + blockIdx.x] = v[0];
+}
+
+// Sum partials [nt][nbx][nq] per slice in a fixed order, then the slices.
+// out[q] = total, slice_out[t*nq + q] = per slice (optional).
+__global__ void k_finalize(const double *__restrict__ part, int nt, int nbx, int nq, double *__restrict__ out,
+                           double *__restrict__ slice_out) {
+    __shared__ double acc[4][256];
+    for (int q = 0; q < nq; q++) acc[q][threadIdx.x] = 0.0;
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        for (int q = 0; q < nq; q++) {
+            double s = 0.0;
+            for (int b = 0; b < nbx; b++) s += part[((size_t)t * nbx + b) * nq + q];
+            if (slice_out) slice_out[(size_t)t * nq + q] = s;
+            acc[q][threadIdx.x] += s;
+        }
+    }
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int q = 0; q < nq; q++) acc[q][threadIdx.x] += acc[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < nq; q++) out[q] = acc[q][0];
+}
+
+int obs_blocks_per_slice(const Lat &l) {
+    uint32_t vsh = l.cb ? l.vs / 2 : l.vs;
+    uint32_t n = vsh * l.npar;
+    int nb = (int)((n + 255) / 256);
+    // enough blocks overall to fill the GPU, not more than one per 256 sites
+    int want = (4 * 148 + l.nt - 1) / l.nt;
+    if (nb > want) nb = want;
+    if (nb < 1) nb = 1;
+    return nb;
+}
+
+void launch_obs(const double2 *u, const Lat &l, double *part, double *out, double *slice_out, cudaStream_t s) {
+    int nbx = obs_blocks_per_slice(l);
+    k_obs_partials<<<dim3(nbx, l.nt), 256, 0, s>>>(u, l, part);
+    k_finalize<<<1, 256, 0, s>>>(part, l.nt, nbx, 2, out, slice_out);
+}
+
+void launch_functional(const double2 *u, const Lat &l, double *part, double *out, cudaStream_t s) {
+    int nbx = obs_blocks_per_slice(l);
+    k_functional_partials<<<dim3(nbx, l.nt), 256, 0, s>>>(u, l, part);
+    k_finalize<<<1, 256, 0, s>>>(part, l.nt, nbx, 1, out, nullptr);
+}
+
+}  // namespace gfc

@@ -1,0 +1,333 @@
+"""ctypes binding of libgfc.so (include/gfc.h), the B200 Coulomb gauge fixer.
+
+The product is the C library and the ``bin/gauge_fix_coulomb`` program; this module
+is the Python view of the same C ABI, used by the tests and the benchmark.  It
+mirrors the reference's in-process interface: ``gaugefix_overrelaxation`` has the
+meaning and return codes of ``gaugefixOverrelaxation`` (gauge_fixing.c:713-826),
+``Params`` is ``ORGaugeFixingParameters`` (gauge_fixing.h:30-54), and the
+observables are ``calculate_e2`` / ``calculateTheta`` / ``calculateF`` /
+``averagePlaquette``.
+
+There is no fallback: if the library is missing, importing this module raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libgfc.so")
+CLI_PATH = os.path.join(_HERE, "bin", "gauge_fix_coulomb")
+
+GFC_OK = 0
+FIX_NOT_CONVERGED = -1
+FIX_BAD_PARAMS = -2
+PROXY_E2, PROXY_THETA = 0, 1
+PREC_FP64_EXACT, PREC_FP64_FAST, PREC_MIXED = 0, 1, 2
+STOP_REFERENCE, STOP_EVERY = 0, 1
+CTX_MIXED = 1
+
+
+class Params(ctypes.Structure):
+    """ORGaugeFixingParameters; omega_OR is a float like the reference's."""
+
+    _fields_ = [
+        ("tolerance", ctypes.c_double),
+        ("gfix_proxy", ctypes.c_int),
+        ("max_sweeps_to_fix", ctypes.c_uint),
+        ("estimate_sweeps_to_gf_progress", ctypes.c_uint),
+        ("sweeps_to_reunitarization", ctypes.c_uint),
+        ("error", ctypes.c_int),
+        ("omega_OR", ctypes.c_float),
+        ("hits", ctypes.c_uint),
+    ]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("precision", ctypes.c_int),
+        ("stop_rule", ctypes.c_int),
+        ("verbose", ctypes.c_int),
+        ("switch_e2", ctypes.c_double),
+        ("refine_reunit", ctypes.c_uint),
+        ("block_threads", ctypes.c_int),
+    ]
+
+
+class Report(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int),
+        ("sweeps", ctypes.c_int),
+        ("sweeps_fp32", ctypes.c_int),
+        ("first_below_tol", ctypes.c_int),
+        ("initial_residue", ctypes.c_double),
+        ("final_residue", ctypes.c_double),
+        ("e2", ctypes.c_double),
+        ("theta", ctypes.c_double),
+        ("functional", ctypes.c_double),
+        ("seconds_sweeps", ctypes.c_double),
+        ("seconds_total", ctypes.c_double),
+        ("site_updates", ctypes.c_longlong),
+        ("kernel_launches", ctypes.c_int),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class GFCError(RuntimeError):
+    pass
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise GFCError(f"{LIB_PATH} is not built (run __graft_entry__.build() or make -C gaugefix-coulomb_b200)")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, I, D, U, S = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_uint, ctypes.c_size_t
+    DP = ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "gfc_params_default": (None, [ctypes.POINTER(Params)]),
+        "gfc_params_valid": (I, [ctypes.POINTER(Params)]),
+        "gfc_params_parse_file": (I, [ctypes.c_char_p, ctypes.POINTER(Params)]),
+        "gfc_params_print": (None, [ctypes.POINTER(Params)]),
+        "gfc_options_default": (None, [ctypes.POINTER(Options)]),
+        "gfc_synth_config": (I, [I, I, ctypes.c_uint64, D, P]),
+        "gfc_read_exact": (I, [ctypes.c_char_p, P, S, I]),
+        "gfc_write_all": (I, [ctypes.c_char_p, P, S]),
+        "gfc_byteswap": (I, [P, S, S]),
+        "gfc_last_error": (ctypes.c_char_p, []),
+        "gfc_host_alloc": (P, [S]),
+        "gfc_host_free": (None, [P]),
+        "gfc_ctx_create": (I, [I, I, I, I, ctypes.POINTER(P)]),
+        "gfc_ctx_destroy": (I, [P]),
+        "gfc_ctx_kernel_launches": (ctypes.c_longlong, [P]),
+        "gfc_ctx_stream": (P, [P]),
+        "gfc_ctx_sync": (I, [P]),
+        "gfc_ctx_upload_links": (I, [P, P, I, I]),
+        "gfc_ctx_download_links": (I, [P, P, I, I]),
+        "gfc_ctx_upload_gt": (I, [P, P, I, I]),
+        "gfc_ctx_download_gt": (I, [P, P, I, I]),
+        "gfc_ctx_get_link": (I, [P, S, I, DP]),
+        "gfc_ctx_reunitarize": (I, [P]),
+        "gfc_ctx_reunitarize_gt": (I, [P]),
+        "gfc_ctx_save_links": (I, [P]),
+        "gfc_ctx_restore_links": (I, [P]),
+        "gfc_ctx_set_identity_gt": (I, [P]),
+        "gfc_ctx_status": (I, [P, ctypes.POINTER(U)]),
+        "gfc_ctx_e2": (I, [P, DP, DP]),
+        "gfc_ctx_e2_slices": (I, [P, P]),
+        "gfc_ctx_functional": (I, [P, DP]),
+        "gfc_ctx_plaquette": (I, [P, DP, DP]),
+        "gfc_ctx_halfsweeps": (I, [P, I, I, ctypes.c_float, U, I]),
+        "gfc_ctx_finalize_temporal": (I, [P]),
+        "gfc_ctx_fix": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), ctypes.POINTER(Report)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error():
+    return lib.gfc_last_error().decode(errors="replace")
+
+
+def _check(rc, what):
+    if rc != GFC_OK:
+        raise GFCError(f"{what} failed ({rc}): {last_error()}")
+
+
+def default_params(**kw):
+    p = Params()
+    lib.gfc_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def parse_params(path):
+    p = Params()
+    lib.gfc_params_parse_file(None if path is None else path.encode(), ctypes.byref(p))
+    return p
+
+
+def options(**kw):
+    o = Options()
+    lib.gfc_options_default(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def synth_config(ns, nt, seed, scale):
+    """Links in the reference layout, float64 array of shape (V*4*18,)."""
+    V = ns ** 3 * nt
+    U = np.empty(V * 4 * 18, dtype=np.float64)
+    _check(lib.gfc_synth_config(ns, nt, seed, scale, U.ctypes.data), "gfc_synth_config")
+    return U
+
+
+class PinnedBuffer:
+    """Page-locked host memory viewed as a numpy array."""
+
+    def __init__(self, nbytes):
+        self.nbytes = int(nbytes)
+        self.ptr = lib.gfc_host_alloc(self.nbytes)
+        if not self.ptr:
+            raise GFCError("gfc_host_alloc failed")
+        self.array = np.ctypeslib.as_array((ctypes.c_uint8 * self.nbytes).from_address(self.ptr))
+
+    def view(self, dtype):
+        return self.array.view(dtype)
+
+    def close(self):
+        if self.ptr:
+            lib.gfc_host_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
+
+
+class Lattice:
+    """One lattice resident on one GPU (a gfc_ctx)."""
+
+    def __init__(self, ns, nt, device=0, mixed=False):
+        self.ns, self.nt = ns, nt
+        self.V = ns ** 3 * nt
+        h = ctypes.c_void_p()
+        _check(lib.gfc_ctx_create(ns, nt, device, CTX_MIXED if mixed else 0, ctypes.byref(h)), "gfc_ctx_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.gfc_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- transfers
+    def upload_links(self, buf, elem_bytes=8, byteswap=False):
+        a = np.ascontiguousarray(buf)
+        assert a.nbytes == self.V * 4 * 18 * elem_bytes, "link buffer size"
+        _check(lib.gfc_ctx_upload_links(self.h, a.ctypes.data, elem_bytes, int(byteswap)), "upload_links")
+
+    def download_links(self, elem_bytes=8, byteswap=False, out=None):
+        dt = np.float64 if elem_bytes == 8 else np.float32
+        out = np.empty(self.V * 4 * 18, dtype=dt) if out is None else out
+        _check(lib.gfc_ctx_download_links(self.h, out.ctypes.data, elem_bytes, int(byteswap)), "download_links")
+        return out
+
+    def upload_gt(self, buf, elem_bytes=8, byteswap=False):
+        a = np.ascontiguousarray(buf)
+        assert a.nbytes == self.V * 18 * elem_bytes
+        _check(lib.gfc_ctx_upload_gt(self.h, a.ctypes.data, elem_bytes, int(byteswap)), "upload_gt")
+
+    def download_gt(self, elem_bytes=8, byteswap=False, out=None):
+        dt = np.float64 if elem_bytes == 8 else np.float32
+        out = np.empty(self.V * 18, dtype=dt) if out is None else out
+        _check(lib.gfc_ctx_download_gt(self.h, out.ctypes.data, elem_bytes, int(byteswap)), "download_gt")
+        return out
+
+    def get_link(self, site, mu):
+        out = (ctypes.c_double * 18)()
+        _check(lib.gfc_ctx_get_link(self.h, site, mu, out), "get_link")
+        return np.array(out[:])
+
+    # ---- fields
+    def reunitarize(self):
+        _check(lib.gfc_ctx_reunitarize(self.h), "reunitarize")
+
+    def reunitarize_gt(self):
+        _check(lib.gfc_ctx_reunitarize_gt(self.h), "reunitarize_gt")
+
+    def save_links(self):
+        _check(lib.gfc_ctx_save_links(self.h), "save_links")
+
+    def restore_links(self):
+        _check(lib.gfc_ctx_restore_links(self.h), "restore_links")
+
+    def set_identity_gt(self):
+        _check(lib.gfc_ctx_set_identity_gt(self.h), "set_identity_gt")
+
+    def status(self):
+        s = ctypes.c_uint()
+        _check(lib.gfc_ctx_status(self.h, ctypes.byref(s)), "status")
+        return s.value
+
+    def halfsweeps(self, first, n, omega=1.95, hits=2, precision=PREC_FP64_EXACT):
+        _check(lib.gfc_ctx_halfsweeps(self.h, first, n, omega, hits, precision), "halfsweeps")
+
+    def finalize_temporal(self):
+        _check(lib.gfc_ctx_finalize_temporal(self.h), "finalize_temporal")
+
+    def sync(self):
+        _check(lib.gfc_ctx_sync(self.h), "sync")
+
+    @property
+    def kernel_launches(self):
+        return lib.gfc_ctx_kernel_launches(self.h)
+
+    @property
+    def stream(self):
+        return lib.gfc_ctx_stream(self.h)
+
+    # ---- observables
+    def e2_theta(self):
+        e2, th = ctypes.c_double(), ctypes.c_double()
+        _check(lib.gfc_ctx_e2(self.h, ctypes.byref(e2), ctypes.byref(th)), "e2")
+        return e2.value, th.value
+
+    def e2_slices(self):
+        out = np.empty(self.nt, dtype=np.float64)
+        _check(lib.gfc_ctx_e2_slices(self.h, out.ctypes.data), "e2_slices")
+        return out
+
+    def functional(self):
+        f = ctypes.c_double()
+        _check(lib.gfc_ctx_functional(self.h, ctypes.byref(f)), "functional")
+        return f.value
+
+    def plaquette(self):
+        s, t = ctypes.c_double(), ctypes.c_double()
+        _check(lib.gfc_ctx_plaquette(self.h, ctypes.byref(s), ctypes.byref(t)), "plaquette")
+        return s.value, t.value
+
+    # ---- the fix
+    def fix(self, params=None, opts=None):
+        """gaugefixOverrelaxation on the resident lattice; returns (rc, report)."""
+        p = params if params is not None else default_params()
+        o = opts if opts is not None else options()
+        r = Report()
+        rc = lib.gfc_ctx_fix(self.h, ctypes.byref(p), ctypes.byref(o), ctypes.byref(r))
+        if rc < FIX_BAD_PARAMS:
+            raise GFCError(f"gfc_ctx_fix failed ({rc}): {last_error()}")
+        return rc, r
+
+
+def gaugefix_overrelaxation(U, G, ns, nt, params=None, opts=None, device=0):
+    """Drop-in of gaugefixOverrelaxation(U, G, params) on host arrays.
+
+    U: float64 array of 4V*18 (reference layout), fixed in place; G: float64 array
+    of V*18, overwritten with the gauge transformation.  Returns the reference's
+    return value (sweeps, -1 or -2) and the run report.
+    """
+    o = opts if opts is not None else options()
+    with Lattice(ns, nt, device=device, mixed=(o.precision == PREC_MIXED)) as lat:
+        lat.upload_links(U, 8, False)
+        rc, rep = lat.fix(params, o)
+        if rc >= 0 or rc == FIX_NOT_CONVERGED:
+            lat.download_links(8, False, out=U)
+            lat.download_gt(8, False, out=G)
+    return rc, rep

@@ -1,0 +1,194 @@
+/*
+ * gfc.h -- C ABI of the B200 Coulomb gauge fixer (libgfc.so).
+ *
+ * Plain pointers and sizes only; no CUDA or torch types cross this boundary, so
+ * the library can be bound from C (the gauge_fix_coulomb CLI), ctypes, cgo or JNI.
+ * Every entry point returns an int status (GFC_OK or a negative GFC_ERR_*), except
+ * the ones that mirror a reference function returning something else; those keep
+ * the reference's return convention and say so.
+ *
+ * Field layouts in HOST memory are the reference's (fields.h:33-43):
+ *   links  U : [t][z][y][x][mu][row][col][re,im], mu = 0 (t), 1 (z), 2 (y), 3 (x)
+ *   gauge  G : [t][z][y][x][row][col][re,im]
+ * i.e. 4V (resp. V) 3x3 complex matrices, V = ns^3 * nt.  Device layouts are
+ * private to the library (structure-of-arrays, checkerboard ordered).
+ */
+#ifndef GFC_H
+#define GFC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------ */
+#define GFC_OK            0
+#define GFC_ERR_ARG      -10   /* bad argument (null pointer, bad size, ...)        */
+#define GFC_ERR_NOMEM    -11   /* host or device allocation failed                  */
+#define GFC_ERR_CUDA     -12   /* a CUDA runtime call failed                        */
+#define GFC_ERR_GEOMETRY -13   /* lattice extents not supported                     */
+#define GFC_ERR_IO       -14   /* file could not be opened / read / written         */
+#define GFC_ERR_STATE    -15   /* call out of order (e.g. fix before upload)        */
+#define GFC_ERR_BUSY     -16   /* serving queue full / no slot                       */
+#define GFC_ERR_TIMEOUT  -17   /* a bounded wait ran out                             */
+#define GFC_ERR_NUMERIC  -18   /* NaN or projection failure reported by a kernel    */
+
+/* gaugefixOverrelaxation return codes (gauge_fixing.c:741-747) */
+#define GFC_FIX_NOT_CONVERGED  -1
+#define GFC_FIX_BAD_PARAMS     -2
+
+/* ---- parameters (gauge_fixing.h:30-54) ---------------------------------------- */
+typedef enum { GFC_PROXY_E2 = 0, GFC_PROXY_THETA = 1 } gfc_proxy;
+
+/* Same members and meaning as ORGaugeFixingParameters; the proxy function pointer
+ * becomes an enum because a host function pointer cannot run on the device.
+ * omega_OR stays a float: the reference stores it as float (gauge_fixing.h:51) and
+ * every update sees (double)(float)omega. */
+typedef struct {
+    double   tolerance;
+    int      gfix_proxy;                     /* gfc_proxy */
+    unsigned max_sweeps_to_fix;
+    unsigned estimate_sweeps_to_gf_progress;
+    unsigned sweeps_to_reunitarization;
+    int      error;                          /* set by the parser on invalid values */
+    float    omega_OR;
+    unsigned hits;
+} gfc_params;
+
+/* Defaults of initParametersORDefault (gauge_fixing.c:72-84). */
+void gfc_params_default(gfc_params *p);
+/* validORGaugeFixingParametersQ (gauge_fixing.c:45-70): 1 if valid, 0 if not. */
+int  gfc_params_valid(const gfc_params *p);
+/* initORGaugeFixingParameters (gauge_fixing.c:144-244): same key:value parser,
+ * same messages on stdout/stderr, accepts the parser's key names and the README /
+ * print-label spellings (max_hits, estimate_sweeps_to_gfixprogress).  path == NULL
+ * or " " means "no file": defaults.  Returns GFC_OK; p->error flags bad values. */
+int  gfc_params_parse_file(const char *path, gfc_params *p);
+/* printORGaugeFixingParameters (gauge_fixing.c:86-104), same text on stdout. */
+void gfc_params_print(const gfc_params *p);
+
+/* ---- run options (no counterpart in the reference: GPU execution choices) ---- */
+typedef enum {
+    GFC_PREC_FP64_EXACT = 0, /* FP64, reference arithmetic: bit-for-bit the reference update */
+    GFC_PREC_FP64_FAST  = 1, /* FP64, direct SU(2) accumulation, FMA                       */
+    GFC_PREC_MIXED      = 2  /* FP32 bulk sweeps, FP64 refinement                           */
+} gfc_precision;
+
+typedef enum {
+    GFC_STOP_REFERENCE = 0,  /* the reference check schedule (gauge_fixing.c:248-285,791-808) */
+    GFC_STOP_EVERY     = 1   /* test the proxy after every half-sweep, stop at first <= tol    */
+} gfc_stop_rule;
+
+typedef struct {
+    int    precision;         /* gfc_precision                                       */
+    int    stop_rule;         /* gfc_stop_rule                                       */
+    int    verbose;           /* print the reference's "Sweeps: ... residue" lines   */
+    double switch_e2;         /* mixed: leave FP32 when e2 < switch_e2 (default 1e-9) */
+    unsigned refine_reunit;   /* mixed: reunitarise every n FP64 half-sweeps (0: use params) */
+    int    block_threads;     /* 0: library default / autotuned                      */
+} gfc_options;
+
+void gfc_options_default(gfc_options *o);
+
+/* ---- run report ------------------------------------------------------------- */
+typedef struct {
+    int    status;            /* return value of the fix                           */
+    int    sweeps;            /* half-sweeps performed                             */
+    int    sweeps_fp32;       /* mixed: half-sweeps done in FP32                   */
+    int    first_below_tol;   /* first half-sweep whose proxy was seen <= tol (-1 if not tracked) */
+    double initial_residue;
+    double final_residue;     /* proxy after the final reunitarisation             */
+    double e2, theta, functional;
+    double seconds_sweeps;    /* device time of the sweep loop                     */
+    double seconds_total;     /* device time of the whole call                     */
+    long long site_updates;   /* sum over half-sweeps of sites updated             */
+    int    kernel_launches;   /* library kernels launched during the call          */
+} gfc_report;
+
+/* ---- synthetic configurations ------------------------------------------------ */
+/* U = 4V matrices (4V*18 doubles, reference layout), built as
+ * U_mu(x) = g(x) exp(i scale H_mu(x)) g(x+mu)^dagger with counter-based seeded
+ * random numbers (see host/gfc_synth.c).  No counterpart in the reference (it
+ * ships no inputs); used by the benchmarks and tests. */
+int gfc_synth_config(int ns, int nt, uint64_t seed, double scale, double *U);
+
+/* ---- host file access (fields_io.c) ------------------------------------------ */
+#define GFC_FILE_CONFIG 0
+#define GFC_FILE_GT     1
+/* Exact-size read with the reference's messages and codes (loadConfig,
+ * fields_io.c:216-305; loadGaugeTransf, fields_io.c:309-402):
+ * 0, -1 cannot open, -2 short read, -3 (config) / -2 (gt) file too long. */
+int gfc_read_exact(const char *path, void *buf, size_t bytes, int kind);
+/* writeGaugeTransf / writeConfig file part (fields_io.c:405-565): 0, -1, -2 */
+int gfc_write_all(const char *path, const void *buf, size_t bytes);
+/* byteSwap (fields_io.c:42-96): reverse every word_bytes (1, 4 or 8) word; -1 otherwise */
+int gfc_byteswap(void *buf, size_t word_bytes, size_t total_bytes);
+
+/* ---- device contexts ------------------------------------------------------------ */
+/* A context holds one lattice resident on one GPU: spatial links, temporal
+ * links, gauge transformation, scratch.  Not thread-safe; one host thread per
+ * context.  No counterpart in the reference, whose state is the global
+ * lattice_param (geometry.h:113-119) plus caller-owned U and G arrays. */
+typedef struct gfc_ctx gfc_ctx;
+#define GFC_CTX_MIXED 1   /* also allocate the FP32 fields and the FP64 copy used by GFC_PREC_MIXED */
+
+const char *gfc_last_error(void);
+/* page-locked host memory for fast transfers (cudaMallocHost / cudaFreeHost) */
+void *gfc_host_alloc(size_t bytes);
+void  gfc_host_free(void *p);
+int  gfc_ctx_create(int ns, int nt, int device, int flags, gfc_ctx **out);
+int  gfc_ctx_destroy(gfc_ctx *c);
+long long gfc_ctx_kernel_launches(const gfc_ctx *c);
+void *gfc_ctx_stream(gfc_ctx *c);   /* the context's cudaStream_t, as void* */
+int  gfc_ctx_sync(gfc_ctx *c);
+
+/* Links in, as raw file bytes in the reference order: elem_bytes 8 (FP64) or 4
+ * (FP32, converted to FP64 like CONV_CFG_TO_WORKING_PRECISION), byteswap 1 for
+ * big-endian files (NEED_BYTE_SWAP_IN).  Pinned host memory is copied directly;
+ * other memory goes through pinned staging.  Swap and conversion run on the GPU. */
+int  gfc_ctx_upload_links(gfc_ctx *c, const void *host, int elem_bytes, int byteswap);
+int  gfc_ctx_download_links(gfc_ctx *c, void *host, int elem_bytes, int byteswap);
+int  gfc_ctx_upload_gt(gfc_ctx *c, const void *host, int elem_bytes, int byteswap);
+int  gfc_ctx_download_gt(gfc_ctx *c, void *host, int elem_bytes, int byteswap);
+
+/* one link (mu = 0 temporal, 1..3 z,y,x) at lexicographic site L, 18 doubles
+ * (getLink, fields.c:233-271) */
+int  gfc_ctx_get_link(gfc_ctx *c, size_t site, int mu, double *out18);
+
+/* reunitarizeField (fields.c:144-187) on all 4V links */
+int  gfc_ctx_reunitarize(gfc_ctx *c);
+/* device-side copy of all links and its restore (restart a fix without a host transfer) */
+int  gfc_ctx_save_links(gfc_ctx *c);
+int  gfc_ctx_restore_links(gfc_ctx *c);
+/* reunitarizeField(G, V) */
+int  gfc_ctx_reunitarize_gt(gfc_ctx *c);
+/* setFieldToIdentity (fields.c:64-100) on G */
+int  gfc_ctx_set_identity_gt(gfc_ctx *c);
+/* device status word (GFC_STATUS_* bits: 1 projection failure, 2 NaN), then cleared */
+int  gfc_ctx_status(gfc_ctx *c, unsigned *status);
+
+/* calculate_e2 / calculateTheta (gauge_fixing.c:341-442), calculateF (289-337),
+ * averagePlaquette spatial / temporal (measurement.c:108-155) */
+int  gfc_ctx_e2(gfc_ctx *c, double *e2, double *theta);
+int  gfc_ctx_e2_slices(gfc_ctx *c, double *e2_per_slice);
+int  gfc_ctx_functional(gfc_ctx *c, double *F);
+int  gfc_ctx_plaquette(gfc_ctx *c, double *spatial, double *temporal);
+
+/* n half-sweeps with indices first_sweep.. (parity = index & 1, as BLACKRED_SWEEP,
+ * gauge_fixing.c:42), no reunitarisation, no stopping test; asynchronous */
+int  gfc_ctx_halfsweeps(gfc_ctx *c, int first_sweep, int n, float omega_OR, unsigned hits, int precision);
+/* apply G to the temporal links (U_t(x) <- G(x) U_t(x) G(x+t)^dagger) and reunitarise them */
+int  gfc_ctx_finalize_temporal(gfc_ctx *c);
+
+/* gaugefixOverrelaxation (gauge_fixing.c:713-826) on the resident lattice:
+ * sets G = 1, fixes U in place (spatial and temporal links), returns the number of
+ * half-sweeps, GFC_FIX_NOT_CONVERGED (-1) or GFC_FIX_BAD_PARAMS (-2); a value below
+ * -2 is a library error (gfc_last_error()).  opt may be NULL (reference behaviour). */
+int  gfc_ctx_fix(gfc_ctx *c, const gfc_params *p, const gfc_options *opt, gfc_report *rep);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GFC_H */

@@ -1,0 +1,546 @@
+/*
+ * ORACLE -- test infrastructure only.
+ *
+ * A CPU restatement, in plain C, of the reference's Coulomb-gauge over-relaxation
+ * (jesuel-marques/GaugeFix-Coulomb, src/gauge_fixing.c and the SU(3)/SU(2)
+ * algebra it calls).  Only tests/, __graft_entry__.smoke() and the cpu_baseline leg
+ * of bench.py may load it, and only as the checker; the product never calls it.
+ *
+ * Arithmetic is written out so that it rounds exactly like the reference build:
+ *   - the reference compiles with -std=c99, which turns FP contraction off, so this
+ *     file is built with -ffp-contract=off (no fused multiply-add);
+ *   - complex products follow the C99 expansion (ac - bd, ad + bc);
+ *   - complex quotients use Smith's method (as libgcc's __divdc3 does for finite,
+ *     normal operands);
+ *   - |z| for a complex z (tgmath fabs) is libm hypot, like cabs;
+ *   - sums accumulate in the reference's loop order, starting from 0.
+ * Parity of this restatement with the reference itself is pinned by the fixtures in
+ * tests/golden/, which were produced by the reference binary built from source
+ * (oracle/Makefile, oracle/ref_harness.c).
+ *
+ * Matrices are 18 doubles, row major, (re, im) pairs.  Link index of the reference
+ * (fields.h:39-43): (((t*ns + z)*ns + y)*ns + x)*4 + mu, mu 0 = t, 1 = z, 2 = y, 3 = x.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct { double re, im; } cplx;
+typedef struct { cplx m[9]; } mat;
+
+static inline cplx cmk(double re, double im) { cplx z = {re, im}; return z; }
+static inline cplx cadd(cplx a, cplx b) { return cmk(a.re + b.re, a.im + b.im); }
+static inline cplx csub(cplx a, cplx b) { return cmk(a.re - b.re, a.im - b.im); }
+static inline cplx cconj(cplx a) { return cmk(a.re, -a.im); }
+static inline cplx cmul(cplx a, cplx b) {
+    return cmk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+/* Smith (1962); for a tiny ratio the operand order of Baudin & Smith (2012). */
+static cplx cdiv(cplx x, cplx y) {
+    double a = x.re, b = x.im, c = y.re, d = y.im, r, den, re, im;
+    if (fabs(c) < fabs(d)) {
+        r = c / d;
+        den = (c * r) + d;
+        if (fabs(r) > 2.2250738585072014e-308) {
+            re = ((a * r) + b) / den;
+            im = ((b * r) - a) / den;
+        } else {
+            re = ((c * (a / d)) + b) / den;
+            im = ((c * (b / d)) - a) / den;
+        }
+    } else {
+        r = d / c;
+        den = (d * r) + c;
+        if (fabs(r) > 2.2250738585072014e-308) {
+            re = ((b * r) + a) / den;
+            im = (b - (a * r)) / den;
+        } else {
+            re = (a + (d * (b / c))) / den;
+            im = (b - (d * (a / c))) / den;
+        }
+    }
+    return cmk(re, im);
+}
+static inline double cabs_(cplx a) { return hypot(a.re, a.im); }
+
+#define E(a, b) ((a) * 3 + (b))
+
+/* ---------------------------------------------------------------- geometry --- */
+typedef struct { int ns, nt; } geo;
+
+static inline size_t site_of(const geo *g, int t, int z, int y, int x) {
+    return (((size_t)t * g->ns + z) * g->ns + y) * g->ns + x;
+}
+/* pos[0] = t, pos[1] = z, pos[2] = y, pos[3] = x (settings.h:57-60) */
+static inline size_t site_pos(const geo *g, const int p[4]) {
+    return site_of(g, p[0], p[1], p[2], p[3]);
+}
+static inline void neighbour(const geo *g, const int p[4], int mu, int dir, int q[4]) {
+    /* geometry.c getNeighbour + makePeriodicBound (mod handles negatives) */
+    memcpy(q, p, 4 * sizeof(int));
+    int n = mu == 0 ? g->nt : g->ns;
+    q[mu] = ((q[mu] + dir) % n + n) % n;
+}
+static inline mat *link(mat *U, const geo *g, const int p[4], int mu) {
+    return U + site_pos(g, p) * 4 + mu;
+}
+
+/* ------------------------------------------------------------ SU(3) algebra -- */
+static void set_identity(mat *u) {
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) u->m[E(a, b)] = cmk(a == b ? 1.0 : 0.0, 0.0);
+}
+
+/* prod3x3 (SU3_ops.c:442-476): uv_ab = sum_c u_ac v_cb, accumulated from 0 */
+static void prod(const mat *u, const mat *v, mat *uv) {
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            cplx s = cmk(0.0, 0.0);
+            for (int c = 0; c < 3; c++) s = cadd(s, cmul(u->m[E(a, c)], v->m[E(c, b)]));
+            uv->m[E(a, b)] = s;
+        }
+}
+
+static void herm_conj(const mat *u, mat *ud) {
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) ud->m[E(a, b)] = cconj(u->m[E(b, a)]);
+}
+
+/* determinant3x3 (SU3_ops.c:251-281), Leibniz form in the reference's order */
+static cplx det3(const mat *u) {
+    const cplx *m = u->m;
+    cplx t0 = cmul(m[E(0, 0)], csub(cmul(m[E(1, 1)], m[E(2, 2)]), cmul(m[E(1, 2)], m[E(2, 1)])));
+    cplx t1 = cmul(m[E(0, 1)], csub(cmul(m[E(1, 2)], m[E(2, 0)]), cmul(m[E(1, 0)], m[E(2, 2)])));
+    cplx t2 = cmul(m[E(0, 2)], csub(cmul(m[E(1, 0)], m[E(2, 1)]), cmul(m[E(1, 1)], m[E(2, 0)])));
+    return cadd(cadd(t0, t1), t2);
+}
+
+/* inverse3x3 (SU3_ops.c:843-900): cofactors divided by the complex determinant.
+   Returns the real part of det (the reference returns a double). */
+static double inverse3(const mat *a, mat *ai) {
+    const cplx *m = a->m;
+    cplx d = det3(a);
+    if (d.re != 0.0 || d.im != 0.0) {
+#define COF(p, q, r, s) csub(cmul(m[p], m[q]), cmul(m[r], m[s]))
+        ai->m[E(0, 0)] = cdiv(COF(E(1, 1), E(2, 2), E(1, 2), E(2, 1)), d);
+        ai->m[E(0, 1)] = cdiv(COF(E(0, 2), E(2, 1), E(0, 1), E(2, 2)), d);
+        ai->m[E(0, 2)] = cdiv(COF(E(0, 1), E(1, 2), E(0, 2), E(1, 1)), d);
+        ai->m[E(1, 0)] = cdiv(COF(E(1, 2), E(2, 0), E(1, 0), E(2, 2)), d);
+        ai->m[E(1, 1)] = cdiv(COF(E(0, 0), E(2, 2), E(0, 2), E(2, 0)), d);
+        ai->m[E(1, 2)] = cdiv(COF(E(0, 2), E(1, 0), E(0, 0), E(1, 2)), d);
+        ai->m[E(2, 0)] = cdiv(COF(E(1, 0), E(2, 1), E(1, 1), E(2, 0)), d);
+        ai->m[E(2, 1)] = cdiv(COF(E(0, 1), E(2, 0), E(0, 0), E(2, 1)), d);
+        ai->m[E(2, 2)] = cdiv(COF(E(0, 0), E(1, 1), E(0, 1), E(1, 0)), d);
+#undef COF
+    } else {
+        for (int k = 0; k < 9; k++) ai->m[k] = cmk(0.0, 0.0);
+    }
+    return d.re;
+}
+
+/* normalize3Vec (SU3_ops.c:903-951): r = sum |v_a|^2 with |.| = cabs */
+static int normalize3(cplx v[3]) {
+    double r = 0.0;
+    for (int a = 0; a < 3; a++) {
+        double h = cabs_(v[a]);
+        r += h * h;
+    }
+    if (r != 0) {
+        r = 1.0 / sqrt(r);
+        for (int a = 0; a < 3; a++) v[a] = cmk(v[a].re * r, v[a].im * r);
+        return 0;
+    }
+    return -1;
+}
+
+/* crossproductConj (SU3_ops.c:954-989) */
+static void cross_conj(const cplx u[3], const cplx v[3], cplx w[3]) {
+    w[0] = cconj(csub(cmul(u[1], v[2]), cmul(u[2], v[1])));
+    w[1] = cconj(csub(cmul(u[2], v[0]), cmul(u[0], v[2])));
+    w[2] = cconj(csub(cmul(u[0], v[1]), cmul(u[1], v[0])));
+}
+
+/* projectSU3 (SU3_ops.c:994-1049): Gram-Schmidt of rows 0,1 + conjugate cross */
+static int project_su3(mat *x) {
+    cplx v0[3], v1[3], v2[3];
+    for (int b = 0; b < 3; b++) {
+        v0[b] = x->m[E(0, b)];
+        v1[b] = x->m[E(1, b)];
+    }
+    int st = normalize3(v0);
+    cross_conj(v0, v1, v2);
+    st |= normalize3(v2);
+    cross_conj(v2, v0, v1);
+    for (int b = 0; b < 3; b++) {
+        x->m[E(0, b)] = v0[b];
+        x->m[E(1, b)] = v1[b];
+        x->m[E(2, b)] = v2[b];
+    }
+    return st == 0 ? 0 : -1;
+}
+
+/* updateSubLosAlamos (SU3_ops.c:776-840) with projectSU2 (SU2_ops.c:369-402) and
+   accumProdSU2_3x3 (SU3_ops.c:636-685).  sub 0 = R (0,1), 1 = S (0,2), 2 = T (1,2). */
+static void sub_los_alamos(mat *w, int sub) {
+    int a = sub == 2 ? 1 : 0;
+    int b = sub == 0 ? 1 : 2;
+    cplx *m = w->m;
+    double ck[4];
+    ck[0] = m[E(a, a)].re + m[E(b, b)].re;
+    ck[1] = -(m[E(a, b)].im + m[E(b, a)].im);
+    ck[2] = -(m[E(a, b)].re - m[E(b, a)].re);
+    ck[3] = -(m[E(a, a)].im - m[E(b, b)].im);
+    double det = 0.0;
+    for (int k = 0; k < 4; k++) det += ck[k] * ck[k];
+    if (det == 0) return;
+    double inv = 1.0 / sqrt(det);
+    for (int k = 0; k < 4; k++) ck[k] = inv * ck[k];
+    /* convertFromCK (SU2_ops.c:94-130) */
+    cplx x00 = cmk(ck[0], ck[3]), x01 = cmk(ck[2], ck[1]);
+    cplx x10 = cmk(-ck[2], ck[1]), x11 = cmk(ck[0], -ck[3]);
+    for (int c = 0; c < 3; c++) {
+        cplx ga = m[E(a, c)], gb = m[E(b, c)];
+        cplx n1 = cadd(cmul(x00, ga), cmul(x01, gb));
+        cplx n2 = cadd(cmul(x10, ga), cmul(x11, gb));
+        m[E(a, c)] = n1;
+        m[E(b, c)] = n2;
+    }
+}
+
+/* ----------------------------------------------------- the local OR update --- */
+/* calculate_w (gauge_fixing.c:445-531): w = sum_{mu spatial} U_mu(x) + U_mu(x-mu)^dag,
+   mu in the order 1 (z), 2 (y), 3 (x). */
+static void calc_w(mat *U, const geo *g, const int p[4], mat *w) {
+    for (int k = 0; k < 9; k++) w->m[k] = cmk(0.0, 0.0);
+    for (int mu = 1; mu <= 3; mu++) {
+        int q[4];
+        neighbour(g, p, mu, -1, q);
+        const mat *f = link(U, g, p, mu), *r = link(U, g, q, mu);
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+                w->m[E(a, b)] = cadd(w->m[E(a, b)], cadd(f->m[E(a, b)], cconj(r->m[E(b, a)])));
+    }
+}
+
+/* updateLosAlamos (gauge_fixing.c:537-596) */
+static void los_alamos(mat *w, unsigned hits, mat *upd) {
+    mat winv;
+    if (inverse3(w, &winv) != 0.0) {
+        for (unsigned h = 1; h <= hits; h++)
+            for (int sub = 0; sub < 3; sub++) sub_los_alamos(w, sub);
+    } else {
+        /* the reference writes the identity and then overwrites it below */
+        set_identity(upd);
+    }
+    prod(w, &winv, upd);
+}
+
+/* power3x3Binomial (SU3_ops.c:734-771) */
+static int power_binomial(const mat *A, double omega, mat *out) {
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            cplx x = A->m[E(a, b)];
+            if (a == b)
+                out->m[E(a, b)] = cmk(1.0 + omega * (x.re - 1.0), omega * x.im);
+            else
+                out->m[E(a, b)] = cmk(omega * x.re, omega * x.im);
+        }
+    return project_su3(out);
+}
+
+/* gaugefixOverrelaxationLocal (gauge_fixing.c:656-708) + updateLocalUG (600-651) */
+static void or_local(mat *U, mat *G, const geo *g, const int p[4], double omega, unsigned hits) {
+    mat w, la, upd, updd, tmp;
+    calc_w(U, g, p, &w);
+    los_alamos(&w, hits, &la);
+    if (power_binomial(&la, omega, &upd)) set_identity(&upd);
+    mat *gx = G + site_pos(g, p);
+    tmp = *gx;
+    prod(&upd, &tmp, gx);
+    herm_conj(&upd, &updd);
+    for (int mu = 0; mu < 4; mu++) {
+        mat *u = link(U, g, p, mu);
+        tmp = *u;
+        prod(&upd, &tmp, u);
+        int q[4];
+        neighbour(g, p, mu, -1, q);
+        mat *ub = link(U, g, q, mu);
+        tmp = *ub;
+        prod(&tmp, &updd, ub);
+    }
+}
+
+/* One half-sweep: sites with even(x) ^ (sweep & 1) (gauge_fixing.c:42,773-787),
+   visited in the reference's t, z, y, x order. */
+void orc_halfsweep(double *Ud, double *Gd, int ns, int nt, int sweep, double omega, unsigned hits) {
+    geo g = {ns, nt};
+    mat *U = (mat *)Ud, *G = (mat *)Gd;
+    for (int t = 0; t < nt; t++)
+        for (int z = 0; z < ns; z++)
+            for (int y = 0; y < ns; y++)
+                for (int x = 0; x < ns; x++) {
+                    int even = !((x ^ y ^ z ^ t) & 1);
+                    if (even ^ (sweep & 1)) {
+                        int p[4] = {t, z, y, x};
+                        or_local(U, G, &g, p, omega, hits);
+                    }
+                }
+}
+
+/* ------------------------------------------------------------ observables --- */
+/* subtractionHermConjTrless3x3 (SU3_ops.c:322-372) then * (-i/2) (four_potential.c:35-66) */
+static void calc_A(const mat *u, mat *A) {
+    mat d;
+    cplx tr = cmk(0.0, 0.0);
+    for (int a = 0; a < 3; a++) {
+        d.m[E(a, a)] = cmk(0.0, 2.0 * u->m[E(a, a)].im);
+        tr = cadd(tr, d.m[E(a, a)]);
+    }
+    tr = cmk(tr.re / 3.0, tr.im / 3.0);
+    for (int a = 0; a < 3; a++) d.m[E(a, a)] = csub(d.m[E(a, a)], tr);
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            if (a != b) d.m[E(a, b)] = csub(u->m[E(a, b)], cconj(u->m[E(b, a)]));
+    /* (-0.5 i) * z  =  (0.5 z.im, -0.5 z.re) */
+    const cplx al = cmk(-0.0, -0.5);
+    for (int k = 0; k < 9; k++) A->m[k] = cmul(al, d.m[k]);
+}
+
+/* divergenceA (four_potential.c:70-113) */
+static void div_A(mat *U, const geo *g, const int p[4], mat *dA) {
+    for (int k = 0; k < 9; k++) dA->m[k] = cmk(0.0, 0.0);
+    for (int mu = 1; mu <= 3; mu++) {
+        int q[4];
+        neighbour(g, p, mu, -1, q);
+        mat A1, A2;
+        calc_A(link(U, g, p, mu), &A1);
+        calc_A(link(U, g, q, mu), &A2);
+        for (int k = 0; k < 9; k++) dA->m[k] = cadd(dA->m[k], csub(A1.m[k], A2.m[k]));
+    }
+}
+
+/* decomposeAlgebraSU3 (SU3_ops.c:1055-1107) */
+static void decompose(const mat *a, double c[9]) {
+    const cplx *m = a->m;
+    c[0] = 0.0;
+    c[1] = m[E(0, 1)].re + m[E(1, 0)].re;
+    c[2] = -m[E(0, 1)].im + m[E(1, 0)].im;
+    c[3] = m[E(0, 0)].re - m[E(1, 1)].re;
+    c[4] = m[E(0, 2)].re + m[E(2, 0)].re;
+    c[5] = -m[E(0, 2)].im + m[E(2, 0)].im;
+    c[6] = m[E(1, 2)].re + m[E(2, 1)].re;
+    c[7] = -m[E(1, 2)].im + m[E(2, 1)].im;
+    c[8] = (m[E(0, 0)].re + m[E(1, 1)].re - 2.0 * m[E(2, 2)].re) / sqrt(3.0);
+}
+
+/* calculate_e2 (gauge_fixing.c:389-442); per-slice partials summed in t order */
+double orc_e2(double *Ud, int ns, int nt, double *per_slice) {
+    geo g = {ns, nt};
+    mat *U = (mat *)Ud;
+    double tot = 0.0;
+    for (int t = 0; t < nt; t++) {
+        double e2 = 0.0;
+        for (int z = 0; z < ns; z++)
+            for (int y = 0; y < ns; y++)
+                for (int x = 0; x < ns; x++) {
+                    int p[4] = {t, z, y, x};
+                    mat dA;
+                    double c[9];
+                    div_A(U, &g, p, &dA);
+                    decompose(&dA, c);
+                    for (int a = 1; a <= 8; a++) e2 += c[a] * c[a];
+                }
+        if (per_slice) per_slice[t] = e2 / ((double)ns * ns * ns);
+        tot += e2;
+    }
+    return tot / ((double)ns * ns * ns * nt);
+}
+
+/* calculateTheta (gauge_fixing.c:341-384) */
+double orc_theta(double *Ud, int ns, int nt) {
+    geo g = {ns, nt};
+    mat *U = (mat *)Ud;
+    cplx th = cmk(0.0, 0.0);
+    for (int t = 0; t < nt; t++)
+        for (int z = 0; z < ns; z++)
+            for (int y = 0; y < ns; y++)
+                for (int x = 0; x < ns; x++) {
+                    int p[4] = {t, z, y, x};
+                    mat dA, dAd, pr;
+                    div_A(U, &g, p, &dA);
+                    herm_conj(&dA, &dAd);
+                    prod(&dA, &dAd, &pr);
+                    th = cadd(th, cadd(cadd(pr.m[0], pr.m[4]), pr.m[8]));
+                }
+    return th.re / (3.0 * ((double)ns * ns * ns * nt));
+}
+
+/* calculateF (gauge_fixing.c:289-337) */
+double orc_functional(double *Ud, int ns, int nt) {
+    geo g = {ns, nt};
+    mat *U = (mat *)Ud;
+    mat acc;
+    for (int k = 0; k < 9; k++) acc.m[k] = cmk(0.0, 0.0);
+    for (int t = 0; t < nt; t++)
+        for (int z = 0; z < ns; z++)
+            for (int y = 0; y < ns; y++)
+                for (int x = 0; x < ns; x++) {
+                    int p[4] = {t, z, y, x};
+                    for (int mu = 1; mu <= 3; mu++) {
+                        const mat *u = link(U, &g, p, mu);
+                        for (int k = 0; k < 9; k++) acc.m[k] = cadd(acc.m[k], u->m[k]);
+                    }
+                }
+    cplx tr = cadd(cadd(acc.m[0], acc.m[4]), acc.m[8]);
+    return tr.re / (double)((double)ns * ns * ns * nt * 3 * 3);
+}
+
+/* TrPlaquette / averagePlaquettegeneric (measurement.c:37-105) */
+static double plaq_generic(mat *U, const geo *g, int mu, int nu) {
+    double sum_re = 0.0;
+    for (int t = 0; t < g->nt; t++)
+        for (int z = 0; z < g->ns; z++)
+            for (int y = 0; y < g->ns; y++)
+                for (int x = 0; x < g->ns; x++) {
+                    int p[4] = {t, z, y, x}, pm[4], pmn[4], pn[4], q1[4], q2[4];
+                    neighbour(g, p, mu, +1, pm);
+                    neighbour(g, pm, nu, +1, pmn);
+                    neighbour(g, p, nu, +1, pn);
+                    mat ua = *link(U, g, p, mu), ub = *link(U, g, pm, nu), uc, ud;
+                    neighbour(g, pmn, mu, -1, q1);
+                    neighbour(g, pn, nu, -1, q2);
+                    herm_conj(link(U, g, q1, mu), &uc);
+                    herm_conj(link(U, g, q2, nu), &ud);
+                    /* prodFour3x3 (SU3_ops.c:522-566): trace of ua ub uc ud */
+                    cplx tr = cmk(0.0, 0.0);
+                    for (int a = 0; a < 3; a++) {
+                        cplx s = cmk(0.0, 0.0);
+                        for (int c = 0; c < 3; c++)
+                            for (int d = 0; d < 3; d++)
+                                for (int e = 0; e < 3; e++)
+                                    s = cadd(s, cmul(cmul(cmul(ua.m[E(a, c)], ub.m[E(c, d)]),
+                                                          uc.m[E(d, e)]), ud.m[E(e, a)]));
+                        tr = cadd(tr, s);
+                    }
+                    sum_re += tr.re / 3.0;
+                }
+    return sum_re / ((double)g->ns * g->ns * g->ns * g->nt);
+}
+
+/* averagePlaquette (measurement.c:108-155): which = 0 spatial, 1 temporal, 2 total */
+double orc_plaquette(double *Ud, int ns, int nt, int which) {
+    geo g = {ns, nt};
+    mat *U = (mat *)Ud;
+    double avg = 0.0;
+    int count = 0;
+    if (which == 2 || which == 1)
+        for (int i = 1; i <= 3; i++) { avg += plaq_generic(U, &g, 0, i); count++; }
+    if (which == 2 || which == 0) {
+        avg += plaq_generic(U, &g, 3, 2); count++;
+        avg += plaq_generic(U, &g, 3, 1); count++;
+        avg += plaq_generic(U, &g, 2, 1); count++;
+    }
+    return avg / (double)count;
+}
+
+/* reunitarizeField (fields.c:144-187): returns 0, or -1 if any projection failed */
+int orc_reunitarize(double *M, size_t n) {
+    int st = 0;
+    for (size_t i = 0; i < n; i++) st |= project_su3((mat *)M + i);
+    return st ? -1 : 0;
+}
+
+void orc_project_su3(double *M) { project_su3((mat *)M); }
+
+/* applyGaugeTransformationU (fields.c:375-435): U'_mu(x) = G(x) U_mu(x) G(x+mu)^dag */
+void orc_apply_gt(double *Ud, const double *Gd, int ns, int nt) {
+    geo g = {ns, nt};
+    mat *U = (mat *)Ud;
+    const mat *G = (const mat *)Gd;
+    for (int t = 0; t < nt; t++)
+        for (int z = 0; z < ns; z++)
+            for (int y = 0; y < ns; y++)
+                for (int x = 0; x < ns; x++) {
+                    int p[4] = {t, z, y, x};
+                    const mat *gx = G + site_pos(&g, p);
+                    for (int mu = 0; mu < 4; mu++) {
+                        int q[4];
+                        neighbour(&g, p, mu, +1, q);
+                        const mat *gy = G + site_pos(&g, q);
+                        mat *u = link(U, &g, p, mu), r;
+                        /* prod_vuwdagger3x3 (SU3_ops.c:703-730) */
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++) {
+                                cplx s = cmk(0.0, 0.0);
+                                for (int c = 0; c < 3; c++)
+                                    for (int d = 0; d < 3; d++)
+                                        s = cadd(s, cmul(cmul(gx->m[E(a, c)], u->m[E(c, d)]),
+                                                         cconj(gy->m[E(b, d)])));
+                                r.m[E(a, b)] = s;
+                            }
+                        *u = r;
+                    }
+                }
+}
+
+/* whenNextConvergenceCheckQ (gauge_fixing.c:248-285) */
+static int next_check(unsigned sweep, double res, double tol, unsigned estimate) {
+    if (res < tol) return (int)sweep;
+    return (int)(sweep + 10 + (unsigned)(estimate * (1.0 - log10(res) / log10(tol))));
+}
+
+/*
+ * gaugefixOverrelaxation (gauge_fixing.c:713-826) with the e2 or theta proxy.
+ * trace (optional, length trace_len) receives e2 after each half-sweep k at
+ * trace[k-1] (the reference evaluates e2 only at scheduled checks; the trace is
+ * extra work used by the per-sweep parity tests).  ftrace likewise gets F.
+ * Returns the sweep count or -1 / -2 like the reference.
+ */
+int orc_fix(double *Ud, double *Gd, int ns, int nt, double tol, int proxy_theta,
+            unsigned max_sweeps, unsigned estimate, unsigned reunit, float omega_f,
+            unsigned hits, double *trace, double *ftrace, int trace_len,
+            double *final_res, int verbose) {
+    if (!(omega_f >= 1 && omega_f < 2 && tol > 0 && reunit > 0)) return -2;
+    size_t V = (size_t)ns * ns * ns * nt;
+    const double omega = (double)omega_f;
+    for (size_t i = 0; i < V; i++) set_identity((mat *)Gd + i);
+#define PROXY(U) (proxy_theta ? orc_theta((U), ns, nt) : orc_e2((U), ns, nt, NULL))
+    int sweep = 0;
+    double res = PROXY(Ud);
+    if (verbose) printf("Sweeps: %8d.\t residue: %3.2E \n", sweep, res);
+    int due = next_check(sweep, res, tol, estimate);
+    int rc = 0;
+    while (res > tol) {
+        orc_halfsweep(Ud, Gd, ns, nt, sweep, omega, hits);
+        sweep++;
+        if (trace && sweep <= trace_len) trace[sweep - 1] = orc_e2(Ud, ns, nt, NULL);
+        if (ftrace && sweep <= trace_len) ftrace[sweep - 1] = orc_functional(Ud, ns, nt);
+        if (sweep == due) {
+            double last = res;
+            res = PROXY(Ud);
+            if (fabs(res - last) / last < 10E-16) {
+                if (verbose) printf("Sweeps: %8d.\t residue: %3.2E \n", sweep, res);
+                rc = -1;
+                break;
+            } else if (res <= tol) {
+                break;
+            } else {
+                if (verbose) printf("Sweeps: %8d.\t residue: %3.2E \n", sweep, res);
+                due = next_check(sweep, res, tol, estimate);
+            }
+        }
+        if (sweep >= (int)max_sweeps) { rc = -1; break; }
+        if (!(sweep % reunit)) {
+            orc_reunitarize(Ud, 4 * V);
+            orc_reunitarize(Gd, V);
+        }
+    }
+    if (rc == 0) {
+        orc_reunitarize(Ud, 4 * V);
+        orc_reunitarize(Gd, V);
+    }
+    if (final_res) *final_res = PROXY(Ud);
+#undef PROXY
+    return rc == 0 ? sweep : rc;
+}

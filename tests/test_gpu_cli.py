@@ -1,0 +1,49 @@
+"""The drop-in program on the GPU against the reference program's recorded output:
+identical stdout text, gauge-transformation bytes and side file."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import gfc
+import oracle_ref as orc
+from conftest import GOLDEN, PKG
+
+pytestmark = pytest.mark.gpu
+CLI = os.path.join(PKG, "bin", "gauge_fix_coulomb")
+
+
+def write_case(c, d):
+    U = gfc.synth_config(c["ns"], c["nt"], c["seed"], c["scale"])
+    (d / f"{c['name']}.cfg").write_bytes(U.astype(">f8" if c["in_bytes"] == 8 else ">f4").tobytes())
+    (d / f"{c['name']}.par").write_text("#generic parameters\n" + "".join(
+        f"{k}:   {v}\n" for k, v in c["params"].items()))
+
+
+@pytest.mark.parametrize("name", ["l4x8", "cfg0_8x16", "l4x8_f32in"])
+def test_cli_matches_reference(cases, tmp_path, name):
+    c = cases[name]
+    write_case(c, tmp_path)
+    env = dict(os.environ)
+    if c["in_bytes"] == 4:
+        env["GFC_CFG_IN"] = "f32"
+    p = subprocess.run([CLI, f"{name}.cfg", f"{name}.gt_cli", str(c["ns"]), str(c["nt"]), f"{name}.par"],
+                       capture_output=True, text=True, cwd=tmp_path, env=env, timeout=600)
+    assert p.returncode == c["cli_exit"], p.stderr
+    assert p.stdout == open(os.path.join(GOLDEN, f"{name}_stdout.txt")).read()
+    assert p.stderr == open(os.path.join(GOLDEN, f"{name}_stderr.txt")).read()
+    G = np.fromfile(tmp_path / f"{name}.gt_cli", dtype=np.float64)
+    assert orc.sha(G) == c["cli_gt_sha256"]
+    side = (tmp_path / f"sweeps_to_gaugefix_{c['ns']}x{c['nt']}.txt").read_text()
+    assert side == c["side_file"]
+
+
+def test_cli_not_converged_exit(cases, tmp_path):
+    c = cases["l4x8_maxsweeps"]
+    write_case(c, tmp_path)
+    p = subprocess.run([CLI, f"{c['name']}.cfg", "g.out", "4", "8", f"{c['name']}.par"], capture_output=True,
+                       text=True, cwd=tmp_path, timeout=300)
+    assert p.returncode == 1
+    assert "could not be gauge-fixed within the maximum number of sweeps" in p.stderr
+    assert not (tmp_path / "g.out").exists()

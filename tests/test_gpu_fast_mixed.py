@@ -1,0 +1,86 @@
+"""The fast FP64 path and the FP32-bulk / FP64-refine path.
+
+They do not round like the reference, so parity is stated through what the fix
+must deliver: e2 <= tolerance, G in SU(3), G U0 G^dagger = the returned links,
+plaquettes unchanged to 1e-13, and the same Coulomb gauge as the oracle (the
+functional F agrees to 1e-10 relative and the half-sweep count to within 1 %)."""
+import numpy as np
+import pytest
+
+import gfc
+import oracle_ref as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def su3_error(G):
+    M = G.reshape(-1, 9, 2)
+    M = (M[..., 0] + 1j * M[..., 1]).reshape(-1, 3, 3)
+    unit = np.abs(M @ M.conj().transpose(0, 2, 1) - np.eye(3)).max()
+    det = np.abs(np.linalg.det(M) - 1).max()
+    return max(unit, det)
+
+
+def first_below(ns, nt, U0, tol, omega=1.95, hits=2):
+    """Half-sweeps until the oracle's e2 first reaches tol (checked every half-sweep)."""
+    U = U0.copy()
+    V = ns ** 3 * nt
+    G = np.zeros(V * 18)
+    G.reshape(V, 9, 2)[:, [0, 4, 8], 0] = 1.0
+    k = 0
+    while orc.e2(U, ns, nt) > tol:
+        orc.halfsweep(U, G, ns, nt, k, omega, hits)
+        k += 1
+        if k % 250 == 0:
+            orc.reunitarize(U)
+            orc.reunitarize(G)
+    return k, U, G
+
+
+@pytest.mark.parametrize("prec", [gfc.PREC_FP64_FAST, gfc.PREC_FP64_EXACT, gfc.PREC_MIXED])
+def test_every_sweep_stopping(prec):
+    ns, nt, tol = 8, 8, 1e-15
+    U0 = gfc.synth_config(ns, nt, 51, 0.5)
+    orc.reunitarize(U0)
+    k_ref, Uref, Gref = first_below(ns, nt, U0, tol)
+    with gfc.Lattice(ns, nt, mixed=(prec == gfc.PREC_MIXED)) as lat:
+        lat.upload_links(U0, 8, False)
+        ps0, pt0 = lat.plaquette()
+        p = gfc.default_params(tolerance=tol)
+        rc, rep = lat.fix(p, gfc.options(precision=prec, stop_rule=gfc.STOP_EVERY))
+        ps1, pt1 = lat.plaquette()
+        G = lat.download_gt()
+        U = lat.download_links()
+        e2, _ = lat.e2_theta()
+    assert rc > 0 and rep.first_below_tol >= 0
+    assert e2 <= tol and rep.final_residue <= tol
+    assert su3_error(G) < 1e-13
+    assert abs(ps1 - ps0) < 1e-13 and abs(pt1 - pt0) < 1e-13
+    # the returned links are G U0 G^dagger
+    U1 = U0.copy()
+    orc.apply_gt(U1, G, ns, nt)
+    np.testing.assert_allclose(U1, U, atol=1e-12)
+    # same gauge functional as the FP64 oracle at its stopping point
+    assert rep.functional == pytest.approx(orc.functional(Uref, ns, nt), rel=1e-10)
+    if prec != gfc.PREC_MIXED:
+        # the fused test sees e2 one half-sweep late (see gfc_fast.cu)
+        assert abs(rep.first_below_tol - k_ref) <= max(1, 0.01 * k_ref)
+
+
+def test_fast_tracks_exact_per_sweep():
+    """The fast update follows the reference update to rounding for many sweeps."""
+    ns, nt = 8, 8
+    U0 = gfc.synth_config(ns, nt, 52, 0.5)
+    orc.reunitarize(U0)
+    out = {}
+    for prec in (gfc.PREC_FP64_EXACT, gfc.PREC_FP64_FAST):
+        with gfc.Lattice(ns, nt) as lat:
+            lat.upload_links(U0, 8, False)
+            lat.set_identity_gt()
+            e2 = []
+            for k in range(200):
+                lat.halfsweeps(k, 1, 1.95, 2, prec)
+                e2.append(lat.e2_theta()[0])
+            out[prec] = (np.array(e2), lat.functional())
+    np.testing.assert_allclose(out[gfc.PREC_FP64_FAST][0], out[gfc.PREC_FP64_EXACT][0], rtol=1e-6)
+    assert out[gfc.PREC_FP64_FAST][1] == pytest.approx(out[gfc.PREC_FP64_EXACT][1], rel=1e-12)

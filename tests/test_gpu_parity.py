@@ -1,0 +1,113 @@
+"""GPU parity with the reference, through the C ABI.
+
+The exact FP64 path (reference arithmetic on the GPU) must return the reference's
+gauge transformation and spatial links bit for bit, the same sweep count and
+return code, the per-half-sweep gauge functional F and e2 to 1e-12 relative, and
+a plaquette unchanged to 1e-13.  Fixtures: tests/golden (made by the reference).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import gfc
+import oracle_ref as orc
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+EXACT_CASES = ["cfg0_8x16", "l4x8", "l4x8_theta", "l4x5_oddnt", "l3x4_oddns", "l5x4_oddns", "l2x4", "l6x6_params",
+               "l4x8_maxsweeps", "l8x8_scale07", "l6x12_hits3"]
+
+
+def raw_config(c):
+    U = gfc.synth_config(c["ns"], c["nt"], c["seed"], c["scale"])
+    return np.frombuffer(U.astype(">f8" if c["in_bytes"] == 8 else ">f4").tobytes(), dtype=np.uint8)
+
+
+def case_params(c, tmp_path):
+    f = tmp_path / "case.par"
+    f.write_text("".join(f"{k}: {v}\n" for k, v in c["params"].items()))
+    return gfc.parse_params(str(f))
+
+
+@pytest.mark.parametrize("name", EXACT_CASES)
+def test_exact_path_bit_for_bit(cases, tmp_path, name):
+    c = cases[name]
+    ns, nt = c["ns"], c["nt"]
+    with gfc.Lattice(ns, nt) as lat:
+        lat.upload_links(raw_config(c), c["in_bytes"], byteswap=True)
+        lat.reunitarize()
+        ps0, pt0 = lat.plaquette()
+        rc, rep = lat.fix(case_params(c, tmp_path), gfc.options(precision=gfc.PREC_FP64_EXACT))
+        assert rc == c["sweeps"]
+        G = lat.download_gt()
+        U = lat.download_links()
+        ps1, pt1 = lat.plaquette()
+    assert orc.sha(G) == c["gt_sha256"], f"max |dG| = {np.abs(G - np.load(os.path.join(GOLDEN, name + '_gt.npy'))).max() if os.path.exists(os.path.join(GOLDEN, name + '_gt.npy')) else 'n/a'}"
+    assert orc.sha(U.reshape(-1, 4, 18)[:, 1:4, :]) == c["u_spatial_sha256"]
+    assert rep.final_residue == pytest.approx(c["final_residue"], rel=1e-12)
+    if rc > 0:
+        assert abs(ps1 - ps0) < 1e-13 and abs(pt1 - pt0) < 1e-13
+        assert ps1 == pytest.approx(c["plaq_spatial"], abs=1e-13)
+        assert pt1 == pytest.approx(c["plaq_temporal"], abs=1e-13)
+
+
+def test_fp32_input_bit_for_bit(cases, tmp_path):
+    c = cases["l4x8_f32in"]
+    with gfc.Lattice(c["ns"], c["nt"]) as lat:
+        lat.upload_links(raw_config(c), 4, byteswap=True)
+        lat.reunitarize()
+        rc, rep = lat.fix(case_params(c, tmp_path))
+        G = lat.download_gt()
+    assert rc == c["cli_sweeps"]
+    assert orc.sha(G) == c["cli_gt_sha256"]
+
+
+@pytest.mark.parametrize("name,nsweeps", [("l4x8", None), ("cfg0_8x16", None), ("l3x4_oddns", 400),
+                                          ("l6x6_params", None)])
+def test_per_half_sweep_functional_and_e2(cases, tmp_path, name, nsweeps):
+    """e2 and F after every half-sweep against the reference's trace (1e-12 rel)."""
+    c = cases[name]
+    ns, nt = c["ns"], c["nt"]
+    trace = np.load(os.path.join(GOLDEN, f"{name}_trace.npy"))
+    n = len(trace) - 1 if nsweeps is None else min(nsweeps, len(trace) - 1)
+    p = case_params(c, tmp_path)
+    e2s, Fs = np.empty(n), np.empty(n)
+    with gfc.Lattice(ns, nt) as lat:
+        lat.upload_links(raw_config(c), 8, byteswap=True)
+        lat.reunitarize()
+        lat.set_identity_gt()
+        e2_0, _ = lat.e2_theta()
+        assert e2_0 == pytest.approx(trace[0, 1], rel=1e-12)
+        assert lat.functional() == pytest.approx(trace[0, 2], rel=1e-12)
+        for k in range(n):
+            lat.halfsweeps(k, 1, p.omega_OR, p.hits, gfc.PREC_FP64_EXACT)
+            e2s[k], _ = lat.e2_theta()
+            Fs[k] = lat.functional()
+            if (k + 1) % p.sweeps_to_reunitarization == 0:
+                lat.reunitarize()
+                lat.reunitarize_gt()
+    np.testing.assert_allclose(e2s, trace[1:n + 1, 1], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(Fs, trace[1:n + 1, 2], rtol=1e-12, atol=0)
+
+
+def test_full_size_halfsweeps_bit_for_bit():
+    """32^3x64 (the FP64 drop-in workload): two exact half-sweeps on the GPU equal
+    the oracle's, bit for bit, for G and the spatial links."""
+    ns, nt = 32, 64
+    U = gfc.synth_config(ns, nt, 2, 0.5)
+    orc.reunitarize(U)
+    V = ns ** 3 * nt
+    G = np.zeros(V * 18)
+    G.reshape(V, 9, 2)[:, [0, 4, 8], 0] = 1.0
+    with gfc.Lattice(ns, nt) as lat:
+        lat.upload_links(U, 8, byteswap=False)
+        lat.set_identity_gt()
+        lat.halfsweeps(0, 2, 1.95, 2, gfc.PREC_FP64_EXACT)
+        Gg = lat.download_gt()
+        Ug = lat.download_links()
+    orc.halfsweep(U, G, ns, nt, 0)
+    orc.halfsweep(U, G, ns, nt, 1)
+    assert orc.sha(Gg) == orc.sha(G)
+    assert orc.sha(Ug.reshape(-1, 4, 18)[:, 1:4, :]) == orc.sha(U.reshape(-1, 4, 18)[:, 1:4, :])
