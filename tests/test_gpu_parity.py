@@ -50,7 +50,12 @@ def test_exact_path_bit_for_bit(cases, tmp_path, name):
     if rc > 0:
         assert abs(ps1 - ps0) < 1e-13 and abs(pt1 - pt0) < 1e-13
         assert ps1 == pytest.approx(c["plaq_spatial"], abs=1e-13)
-        assert pt1 == pytest.approx(c["plaq_temporal"], abs=1e-13)
+        if nt % 2 == 0:
+            assert pt1 == pytest.approx(c["plaq_temporal"], abs=1e-13)
+        # With odd nt the reference's threads for t = 0 and t = nt-1 update the same
+        # boundary temporal links concurrently (gauge_fixing.c:638-650 under the
+        # OpenMP loop at 773), so its temporal plaquette after fixing is not the
+        # gauge-invariant value; ours stays equal to the value before (checked above).
 
 
 def test_fp32_input_bit_for_bit(cases, tmp_path):
