@@ -121,6 +121,7 @@ def _load():
         "gfc_ctx_halfsweeps": (I, [P, I, I, ctypes.c_float, U, I]),
         "gfc_ctx_finalize_temporal": (I, [P]),
         "gfc_ctx_fix": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), ctypes.POINTER(Report)]),
+        "gfc_e2_theta_device_noalloc": (I, [I, I, P, P, DP, DP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -182,6 +182,22 @@ int  gfc_ctx_halfsweeps(gfc_ctx *c, int first_sweep, int n, float omega_OR, unsi
 /* apply G to the temporal links (U_t(x) <- G(x) U_t(x) G(x+t)^dagger) and reunitarise them */
 int  gfc_ctx_finalize_temporal(gfc_ctx *c);
 
+/* ---- allocation-free observable --------------------------------------------------- */
+/* e2 and theta (the quantities of gfc_ctx_e2) of links the caller already holds in
+ * device memory on the current device, in the reference layout (4V*18 doubles),
+ * without allocating any device memory: for callers that cannot let a library call
+ * cudaMalloc/cudaFree (their allocator owns the GPU's memory, or a device-wide
+ * synchronisation from cudaFree would stall other work sharing the GPU).  No
+ * counterpart in the reference.  Scratch is a fixed 128 KiB array inside the
+ * library (GFC_NOALLOC_SCRATCH_DOUBLES doubles per GPU, held until exit); lattices
+ * whose partial sums do not fit are rejected with GFC_ERR_ARG and a message in
+ * gfc_last_error().  Calls share that array: calls that overlap on the GPU race.
+ * The first call on a device looks up the array's address; make it before any
+ * stream capture.  stream is a cudaStream_t (NULL: the legacy default stream);
+ * the call waits for its own result. */
+#define GFC_NOALLOC_SCRATCH_DOUBLES 16384
+int  gfc_e2_theta_device_noalloc(int ns, int nt, const double *u_dev, void *stream, double *e2, double *theta);
+
 /* gaugefixOverrelaxation (gauge_fixing.c:713-826) on the resident lattice:
  * sets G = 1, fixes U in place (spatial and temporal links), returns the number of
  * half-sweeps, GFC_FIX_NOT_CONVERGED (-1) or GFC_FIX_BAD_PARAMS (-2); a value below
