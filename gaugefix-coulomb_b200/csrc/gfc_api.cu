@@ -50,6 +50,8 @@ static void ctx_free(gfc_ctx *c) {
     cudaFree(c->ut);
     cudaFree(c->u0);
     cudaFree(c->backup);
+    cudaFree(c->u64r);
+    cudaFree(c->g64r);
     cudaFree(c->u32);
     cudaFree(c->g32);
     cudaFree(c->part);
@@ -58,6 +60,7 @@ static void ctx_free(gfc_ctx *c) {
     cudaFree(c->e2_slice);
     cudaFree(c->e2_hist);
     cudaFree(c->tickets);
+    cudaFree(c->ring);
     for (int k = 0; k < 2; k++) {
         cudaFree(c->dstage[k]);
         cudaFreeHost(c->hstage[k]);
@@ -467,13 +470,14 @@ extern "C" int gfc_ctx_halfsweeps(gfc_ctx *c, int first_sweep, int n, float omeg
     if (!c->has_links) return GFC_ERR_STATE;
     GFC_CHECK(cudaSetDevice(c->dev));
     const double omega = (double)omega_OR;
-    for (int k = 0; k < n; k++) {
-        int sw = first_sweep + k;
-        if (precision == GFC_PREC_FP64_EXACT || !c->lat.cb)
-            launch_sweep_exact(c->u, c->g, c->lat, sw, omega, hits, c->s);
-        else
-            launch_sweep_fast64(c, sw, omega, hits, 0);
-        c->launches++;
+    if (precision == GFC_PREC_FP64_EXACT || !c->lat.cb) {
+        for (int k = 0; k < n; k++) {
+            launch_sweep_exact(c->u, c->g, c->lat, first_sweep + k, omega, hits, c->s, c->shape_exact);
+            c->launches++;
+        }
+    } else if (n > 0) {
+        int rc = halfsweeps_fast64(c, first_sweep, n, omega, hits);
+        if (rc) return rc;
     }
     GFC_CHECK(cudaGetLastError());
     return GFC_OK;
@@ -527,12 +531,22 @@ static int fix_reference_schedule(gfc_ctx *c, const gfc_params *p, const gfc_opt
     int due = next_check(sweep, res, p);
     GFC_CHECK(cudaEventRecord(c->ev_b, c->s));
     while (res > p->tolerance) {
-        if (o->precision == GFC_PREC_FP64_EXACT || !l.cb)
-            launch_sweep_exact(c->u, c->g, l, sweep, omega, p->hits, c->s);
-        else
-            launch_sweep_fast64(c, sweep, omega, p->hits, 0);
-        c->launches++;
-        sweep++;
+        // half-sweeps up to the next event (scheduled check, max_sweeps, reunitarisation);
+        // none of the tests below can fire on the half-sweeps in between
+        int n = due - sweep;
+        n = std::min(n, (int)p->max_sweeps_to_fix - sweep);
+        n = std::min(n, (int)(p->sweeps_to_reunitarization - sweep % p->sweeps_to_reunitarization));
+        n = std::max(n, 1);
+        if (o->precision == GFC_PREC_FP64_EXACT || !l.cb) {
+            for (int k = 0; k < n; k++) {
+                launch_sweep_exact(c->u, c->g, l, sweep + k, omega, p->hits, c->s, c->shape_exact);
+                c->launches++;
+            }
+        } else {
+            e = halfsweeps_fast64(c, sweep, n, omega, p->hits);
+            if (e) return e;
+        }
+        sweep += n;
         if (sweep == due) {
             double last = res;
             e = proxy(c, p, &res);
@@ -574,7 +588,7 @@ static int fix_every_sweep_exact(gfc_ctx *c, const gfc_params *p, const gfc_opti
     GFC_CHECK(cudaEventRecord(c->ev_b, c->s));
     if (res <= p->tolerance) rc = 0;
     while (rc != 0 && sweep < (int)p->max_sweeps_to_fix) {
-        launch_sweep_exact(c->u, c->g, l, sweep, omega, p->hits, c->s);
+        launch_sweep_exact(c->u, c->g, l, sweep, omega, p->hits, c->s, c->shape_exact);
         c->launches++;
         sweep++;
         e = proxy(c, p, &res);

@@ -17,6 +17,8 @@ struct gfc_ctx {
     double2 *ut = nullptr;        // temporal links
     double2 *u0 = nullptr;        // copy of the spatial links at the start of a mixed fix
     void *backup = nullptr;       // gfc_ctx_save_links copy (spatial + temporal)
+    double2 *u64r = nullptr;      // fast FP64 sweeps: links, rows 0 and 1 only
+    double2 *g64r = nullptr;      // fast FP64 sweeps: G, rows 0 and 1 only
     // FP32 fields for the mixed-precision bulk (two stored rows per link)
     float2 *u32 = nullptr;
     float2 *g32 = nullptr;
@@ -38,6 +40,18 @@ struct gfc_ctx {
     unsigned *tickets = nullptr;  // [nt + 2]: per-slice and global tickets, stop word
     int has_links = 0;
     long long launches = 0;
+    // launch shapes of the sweep kernels (indices into the compiled shape tables;
+    // defaults until gfc_ctx_autotune measures them for this lattice)
+    int shape_exact = 1;
+    int shape_fast64 = 1;
+    int shape_fast32 = 2;
+    int tuned = 0;
+    // slice blocking of the fast sweeps: groups of blk*_slices timeslices run
+    // blk*_sweeps half-sweeps each while resident in L2 (0 / 1: not blocked)
+    int blk64_slices = 0, blk64_sweeps = 1;
+    int blk32_slices = 0, blk32_sweeps = 1;
+    double *ring = nullptr;       // per-slice e2 partials of the last half-sweeps
+    int ring_n = 0;
 };
 
 namespace gfc {

@@ -112,6 +112,31 @@ struct S64 {
         for (int c = 0; c < 9; c++) p[(size_t)c * st] = m.e[c];
     }
     static constexpr bool ROWS01_ONLY = false;
+    static constexpr bool ROWWISE = true;
+    static constexpr int STORED_ROWS = 3;
+};
+
+// FP64, rows 0 and 1 only (6 double2 per matrix, 96 B); row 2 rebuilt as conj(r0 x r1)
+struct S64R {
+    using T = double;
+    using V = double2;
+    static constexpr int NS = 6;
+    static constexpr int BYTES = 96;
+    __device__ static void load_rows01(const V *__restrict__ p, size_t st, Mt<T> &m) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) m.e[c] = p[(size_t)c * st];
+    }
+    __device__ static void load(const V *__restrict__ p, size_t st, Mt<T> &m) {
+        load_rows01(p, st, m);
+        reconstruct_row2(m);
+    }
+    __device__ static void store(V *__restrict__ p, size_t st, const Mt<T> &m) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) p[(size_t)c * st] = m.e[c];
+    }
+    static constexpr bool ROWS01_ONLY = true;
+    static constexpr bool ROWWISE = true;
+    static constexpr int STORED_ROWS = 2;
 };
 
 struct S32 {
@@ -138,6 +163,8 @@ struct S32 {
         p[2 * st] = make_float4(m.e[4].x, m.e[4].y, m.e[5].x, m.e[5].y);
     }
     static constexpr bool ROWS01_ONLY = true;
+    static constexpr bool ROWWISE = false;
+    static constexpr int STORED_ROWS = 2;
 };
 
 template <class S>
@@ -271,16 +298,163 @@ __device__ __forceinline__ void fprod_dag(const Mt<T> &a, const Mt<T> &b, Mt<T> 
         }
 }
 
+// Contribution of row i = (o0, o1, o2) of a matrix o added to w (sign +1) or of
+// o^dagger added to w (sign -1) to the 8 algebra components of w's e2 density:
+//   c1 = Im w01 + Im w10, c2 = Re w01 - Re w10, c3 = Im w00 - Im w11,
+//   c4 = Im w02 + Im w20, c5 = Re w02 - Re w20, c6 = Im w12 + Im w21,
+//   c7 = Re w12 - Re w21, c8 = Im w00 + Im w11 - 2 Im w22 (times 1/sqrt 3 later).
+// Adding o^dagger contributes exactly the negative of adding o.
+template <int I, typename C>
+__device__ __forceinline__ void acc_row(double (&c)[8], C o0, C o1, C o2, double s) {
+    if (I == 0) {
+        c[0] += s * o1.y;
+        c[1] += s * o1.x;
+        c[2] += s * o0.y;
+        c[3] += s * o2.y;
+        c[4] += s * o2.x;
+        c[7] += s * o0.y;
+    } else if (I == 1) {
+        c[0] += s * o0.y;
+        c[1] -= s * o0.x;
+        c[2] -= s * o1.y;
+        c[5] += s * o2.y;
+        c[6] += s * o2.x;
+        c[7] += s * o1.y;
+    } else {
+        c[3] += s * o0.y;
+        c[4] -= s * o0.x;
+        c[5] += s * o1.y;
+        c[6] -= s * o1.x;
+        c[7] -= 2.0 * s * o2.y;
+    }
+}
+
+template <int I, typename T>
+__device__ __forceinline__ void acc_mat_row(double (&c)[8], const Mt<T> &o, double s) {
+    acc_row<I>(c, o.e[EL(I, 0)], o.e[EL(I, 1)], o.e[EL(I, 2)], s);
+}
+
+// f <- up . f for a forward link; FP64 works one row at a time to keep few values live
+template <class S>
+__device__ __forceinline__ void apply_forward(typename S::V *__restrict__ p, size_t st,
+                                              const Mt<typename S::T> &up, int track, double (&cc)[8]) {
+    using T = typename S::T;
+    using C = typename CT<T>::t;
+    Mt<T> f;
+    S::load(p, st, f);
+    if constexpr (S::ROWWISE) {
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (r >= S::STORED_ROWS && !track) break;   // row 2 of a two-row link: e2 only
+            C o[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C s = fmul(up.e[EL(r, 0)], f.e[EL(0, j)]);
+                s = fadd(s, fmul(up.e[EL(r, 1)], f.e[EL(1, j)]));
+                s = fadd(s, fmul(up.e[EL(r, 2)], f.e[EL(2, j)]));
+                o[j] = s;
+                if (r < S::STORED_ROWS) p[(size_t)(3 * r + j) * st] = s;
+            }
+            if (track) {
+                if (r == 0) acc_row<0>(cc, o[0], o[1], o[2], 1.0);
+                if (r == 1) acc_row<1>(cc, o[0], o[1], o[2], 1.0);
+                if (r == 2) acc_row<2>(cc, o[0], o[1], o[2], 1.0);
+            }
+        }
+    } else {
+        Mt<T> o;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C s = fmul(up.e[EL(r, 0)], f.e[EL(0, j)]);
+                s = fadd(s, fmul(up.e[EL(r, 1)], f.e[EL(1, j)]));
+                s = fadd(s, fmul(up.e[EL(r, 2)], f.e[EL(2, j)]));
+                o.e[EL(r, j)] = s;
+            }
+        S::store(p, st, o);
+        if (track) {
+            acc_mat_row<0>(cc, o, 1.0);
+            acc_mat_row<1>(cc, o, 1.0);
+            acc_mat_row<2>(cc, o, 1.0);
+        }
+    }
+}
+
+// r <- r . up^dagger for a backward link (row-local)
+template <class S>
+__device__ __forceinline__ void apply_backward(typename S::V *__restrict__ p, size_t st,
+                                               const Mt<typename S::T> &up, int track, double (&cc)[8]) {
+    using T = typename S::T;
+    using C = typename CT<T>::t;
+    if constexpr (S::ROWWISE) {
+        C rows[3][3];   // rows of the old link; row 2 of a two-row link is rebuilt for e2
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (r >= S::STORED_ROWS) {
+                if (!track) break;
+                fcross_conj(rows[0], rows[1], rows[2]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 3; j++) rows[r][j] = p[(size_t)(3 * r + j) * st];
+            }
+            const C a0 = rows[r][0], a1 = rows[r][1], a2 = rows[r][2];
+            C o[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C s = fmul_conj(a0, up.e[EL(j, 0)]);
+                s = fadd(s, fmul_conj(a1, up.e[EL(j, 1)]));
+                s = fadd(s, fmul_conj(a2, up.e[EL(j, 2)]));
+                o[j] = s;
+                if (r < S::STORED_ROWS) p[(size_t)(3 * r + j) * st] = s;
+            }
+            if (track) {
+                if (r == 0) acc_row<0>(cc, o[0], o[1], o[2], -1.0);
+                if (r == 1) acc_row<1>(cc, o[0], o[1], o[2], -1.0);
+                if (r == 2) acc_row<2>(cc, o[0], o[1], o[2], -1.0);
+            }
+        }
+    } else {
+        Mt<T> m, o;
+        if (track)
+            S::load(p, st, m);
+        else
+            S::load_rows01(p, st, m);
+        const int nr = track ? 3 : 2;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (r >= nr) break;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C s = fmul_conj(m.e[EL(r, 0)], up.e[EL(j, 0)]);
+                s = fadd(s, fmul_conj(m.e[EL(r, 1)], up.e[EL(j, 1)]));
+                s = fadd(s, fmul_conj(m.e[EL(r, 2)], up.e[EL(j, 2)]));
+                o.e[EL(r, j)] = s;
+            }
+        }
+        S::store(p, st, o);
+        if (track) {
+            acc_mat_row<0>(cc, o, -1.0);
+            acc_mat_row<1>(cc, o, -1.0);
+            acc_mat_row<2>(cc, o, -1.0);
+        }
+    }
+}
+
 // ----------------------------------------------------------- sweep kernel --
 struct SweepArgs {
     Lat l;
     int par;
     double omega;
     unsigned hits;
-    int track;          // 1: compute fused e2 partials
+    int track;          // 0: none; 1: per-slice + whole-lattice sums and stop test
+                        // (grid covers all slices); 2: per-slice sums into the ring only
+    int t0;             // first timeslice of this launch (grid.y slices from t0)
     double *part;       // [nt][nbx][2]
     unsigned *tickets;  // [nt + 1]
     double *slice;      // [nt][2] latest per-slice (pre, post) sums
+    double *ring;       // track 2: [ring_n][nt][2] per-slice sums by half-sweep index
+    int ring_n;
     double *hist;       // [2 * hist_n]: (pre, post) totals per sweep index
     int sweep;          // this half-sweep's index
     int hist_n;
@@ -289,11 +463,20 @@ struct SweepArgs {
     unsigned *status;
 };
 
-constexpr int SWEEP_BLOCK = 128;
+// Launch shapes compiled into the library: (threads per block, minimum resident
+// blocks per SM).  The second number caps registers per thread (65536 / (block *
+// minb)); which shape is fastest depends on the lattice and is measured by
+// gfc_ctx_autotune.
+struct Shape {
+    int block, minb;
+};
+constexpr Shape kShapes[] = {{128, 2}, {128, 3}, {128, 4}, {64, 4}, {64, 6}, {256, 1}, {256, 2}};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+constexpr int MIN_BLOCK = 64;   // smallest block: sizes the per-block partial buffers
 
 // deterministic sum of NQ values over the block; result in thread 0
-template <int NQ>
-__device__ __forceinline__ void fblock_sum(double (&v)[NQ], double (*sh)[SWEEP_BLOCK / 32]) {
+template <int BLOCK, int NQ>
+__device__ __forceinline__ void fblock_sum(double (&v)[NQ], double (*sh)[BLOCK / 32]) {
 #pragma unroll
     for (int q = 0; q < NQ; q++)
 #pragma unroll
@@ -308,19 +491,20 @@ __device__ __forceinline__ void fblock_sum(double (&v)[NQ], double (*sh)[SWEEP_B
         for (int q = 0; q < NQ; q++) {
             double s = 0.0;
 #pragma unroll
-            for (int k = 0; k < SWEEP_BLOCK / 32; k++) s += sh[q][k];
+            for (int k = 0; k < BLOCK / 32; k++) s += sh[q][k];
             v[q] = s;
         }
 }
 
 // Combine block partials: last block of a slice sums the slice, last slice sums
 // all slices, applies the stopping test.  Called by all threads of the block.
+template <int BLOCK>
 __device__ void fused_reduce(const SweepArgs &a, double pre, double post) {
-    __shared__ double sh[2][SWEEP_BLOCK / 32];
+    __shared__ double sh[2][BLOCK / 32];
     __shared__ int last;
     double v[2] = {pre, post};
-    fblock_sum<2>(v, sh);
-    const uint32_t t = blockIdx.y, nbx = gridDim.x, nt = gridDim.y;
+    fblock_sum<BLOCK, 2>(v, sh);
+    const uint32_t t = a.t0 + blockIdx.y, nbx = gridDim.x, nt = gridDim.y;
     if (threadIdx.x == 0) {
         size_t o = ((size_t)t * nbx + blockIdx.x) * 2;
         a.part[o] = v[0];
@@ -339,12 +523,20 @@ __device__ void fused_reduce(const SweepArgs &a, double pre, double post) {
             s0 += __ldcg(p + 2 * b);
             s1 += __ldcg(p + 2 * b + 1);
         }
-        a.slice[2 * t] = s0;
-        a.slice[2 * t + 1] = s1;
         a.tickets[t] = 0;
-        __threadfence();
-        unsigned tk = atomicAdd(&a.tickets[nt], 1u);
-        last = tk == nt - 1;
+        if (a.track == 2) {
+            // slice-blocked sweeping: the whole-lattice test runs after the round
+            double *r = a.ring + ((size_t)(a.sweep % a.ring_n) * a.l.nt + t) * 2;
+            r[0] = s0;
+            r[1] = s1;
+            last = 0;
+        } else {
+            a.slice[2 * t] = s0;
+            a.slice[2 * t + 1] = s1;
+            __threadfence();
+            unsigned tk = atomicAdd(&a.tickets[nt], 1u);
+            last = tk == nt - 1;
+        }
     }
     __syncthreads();
     if (!last || threadIdx.x != 0) return;
@@ -369,20 +561,20 @@ __device__ void fused_reduce(const SweepArgs &a, double pre, double post) {
     }
 }
 
-template <class S>
-__global__ void __launch_bounds__(SWEEP_BLOCK) k_sweep_fast(typename S::V *__restrict__ u,
+template <class S, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_sweep_fast(typename S::V *__restrict__ u,
                                                             typename S::V *__restrict__ g, SweepArgs a) {
     using T = typename S::T;
     using C = typename CT<T>::t;
     if (a.stop && *(volatile unsigned *)a.stop) return;
     const Lat &l = a.l;
     const uint32_t vsh = l.vs >> 1;
-    const uint32_t off = blockIdx.x * SWEEP_BLOCK + threadIdx.x;
+    const uint32_t off = blockIdx.x * BLOCK + threadIdx.x;
     const bool active = off < vsh;
     double pre = 0.0, post = 0.0;
     if (active) {
         const int par = a.par, op = par ^ 1;
-        const uint32_t i = blockIdx.y * vsh + off;
+        const uint32_t i = (a.t0 + blockIdx.y) * vsh + off;
         Coord c = coord_cb(l, par, i);
         uint32_t ib[3];
 #pragma unroll
@@ -406,48 +598,38 @@ __global__ void __launch_bounds__(SWEEP_BLOCK) k_sweep_fast(typename S::V *__res
         Mt<T> up;
         fupdate(w, (T)a.omega, a.hits, up);
 
-        Mt<T> m, o;
-        S::load(g + sg_idx<S>(l, par, i), l.vh, m);
-        fprod_left<S>(up, m, o);
-        S::store(g + sg_idx<S>(l, par, i), l.vh, o);
-#pragma unroll
-        for (int k = 0; k < 9; k++) w.e[k] = mkc<C>(T(0), T(0));
+        // G(x) <- up G(x)
+        {
+            Mt<T> m, o;
+            S::load(g + sg_idx<S>(l, par, i), l.vh, m);
+            fprod_left<S>(up, m, o);
+            S::store(g + sg_idx<S>(l, par, i), l.vh, o);
+        }
+        // links; the post-update w(x) enters e2 only through its 8 algebra
+        // components, accumulated row by row (see acc_row)
+        double cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            S::load(u + su_idx<S>(l, d, par, i), l.vh, m);
-            fprod_left<S>(up, m, o);
-            S::store(u + su_idx<S>(l, d, par, i), l.vh, o);
-            if (a.track) {
-                if (S::ROWS01_ONLY) reconstruct_row2(o);
-#pragma unroll
-                for (int k = 0; k < 9; k++) w.e[k] = fadd(w.e[k], o.e[k]);
-            }
-            // right multiplication is row-local: two-row storage needs no rebuild
-            if (S::ROWS01_ONLY)
-                S::load_rows01(u + su_idx<S>(l, d, op, ib[d]), l.vh, m);
-            else
-                S::load(u + su_idx<S>(l, d, op, ib[d]), l.vh, m);
-            fprod_dag<S>(m, up, o);
-            S::store(u + su_idx<S>(l, d, op, ib[d]), l.vh, o);
-            if (a.track) {
-                if (S::ROWS01_ONLY) reconstruct_row2(o);
-#pragma unroll
-                for (int x = 0; x < 3; x++)
-#pragma unroll
-                    for (int y = 0; y < 3; y++) w.e[EL(x, y)] = fadd(w.e[EL(x, y)], fconj(o.e[EL(y, x)]));
-            }
+            apply_forward<S>(u + su_idx<S>(l, d, par, i), l.vh, up, a.track, cc);
+            apply_backward<S>(u + su_idx<S>(l, d, op, ib[d]), l.vh, up, a.track, cc);
         }
-        if (a.track) post = e2_from_w(w);
+        if (a.track) {
+            cc[7] *= 0.57735026918962576451;
+#pragma unroll
+            for (int k = 0; k < 8; k++) post += cc[k] * cc[k];
+        }
     }
-    if (a.track) fused_reduce(a, pre, post);
+    if (a.track) fused_reduce<BLOCK>(a, pre, post);
 }
 
+// projectSU3 on entries [begin, begin + count) of each of nblk SoA blocks
 template <class S>
-__global__ void k_reunit_fast(typename S::V *__restrict__ base, uint32_t stride, uint32_t nblk,
-                              const unsigned *stop, unsigned *status) {
+__global__ void k_reunit_fast(typename S::V *__restrict__ base, uint32_t stride, uint32_t nblk, uint32_t begin,
+                              uint32_t count, const unsigned *stop, unsigned *status) {
     if (stop && *(volatile const unsigned *)stop) return;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
-    if (i >= stride || k >= nblk) return;
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+    if (j >= count || k >= nblk) return;
+    uint32_t i = begin + j;
     typename S::V *p = base + (size_t)k * S::NS * stride + i;
     Mt<typename S::T> m;
     S::load(p, stride, m);
@@ -488,6 +670,56 @@ __global__ void k_to_f64(const float4 *__restrict__ src, double2 *__restrict__ d
     for (int e = 0; e < 9; e++) q[(size_t)e * stride] = m.e[e];
 }
 
+// FP64 full SoA ([9][stride] per block) -> FP64 two-row SoA ([6][stride])
+__global__ void k_pack2(const double2 *__restrict__ src, double2 *__restrict__ dst, uint32_t stride, uint32_t nblk) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+    if (i >= stride || k >= nblk) return;
+    const double2 *p = src + (size_t)k * 9 * stride + i;
+    double2 *q = dst + (size_t)k * 6 * stride + i;
+#pragma unroll
+    for (int e = 0; e < 6; e++) q[(size_t)e * stride] = p[(size_t)e * stride];
+}
+
+// FP64 two-row -> full, row 2 = conj(row0 x row1)
+__global__ void k_unpack2(const double2 *__restrict__ src, double2 *__restrict__ dst, uint32_t stride, uint32_t nblk) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+    if (i >= stride || k >= nblk) return;
+    Mt<double> m;
+    S64R::load(src + (size_t)k * 6 * stride + i, stride, m);
+    S64::store(dst + (size_t)k * 9 * stride + i, stride, m);
+}
+
+// Slice-blocked sweeping: after a round, e2 after s half-sweeps is
+// sum_t post[s-1][t] + pre[s][t] from the per-slice ring.  Summed in slice order
+// (deterministic).  Sets stop = 0x40000000 | s at the first s with e2 <= tol.
+__global__ void k_round_check(const double *__restrict__ ring, int ring_n, int nt, int s_lo, int s_hi,
+                              double *__restrict__ hist, int hist_n, double tol_sum, unsigned *stop,
+                              unsigned *status) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (*(volatile unsigned *)stop) return;
+    for (int s = s_lo; s <= s_hi; s++) {
+        const double *po = ring + (size_t)((s - 1) % ring_n) * nt * 2;
+        const double *pr = ring + (size_t)(s % ring_n) * nt * 2;
+        double a = 0.0, b = 0.0;
+        for (int t = 0; t < nt; t++) {
+            a += pr[2 * t];
+            b += po[2 * t + 1];
+        }
+        if (s < hist_n) hist[2 * s] = a;
+        if (s - 1 < hist_n) hist[2 * (s - 1) + 1] = b;
+        double e2 = a + b;
+        if (!(e2 == e2)) {
+            atomicOr(status, GFC_STATUS_NAN);
+            *stop = 0x80000000u | (unsigned)s;
+            return;
+        }
+        if (e2 <= tol_sum) {
+            *stop = 0x40000000u | (unsigned)s;
+            return;
+        }
+    }
+}
+
 __global__ void k_identity32(float4 *__restrict__ g, uint32_t stride, uint32_t nblk) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
     if (i >= stride || k >= nblk) return;
@@ -500,7 +732,7 @@ __global__ void k_identity32(float4 *__restrict__ g, uint32_t stride, uint32_t n
 // ------------------------------------------------------------------ host --
 static int ensure_track_buffers(gfc_ctx *c, int hist_n) {
     const Lat &l = c->lat;
-    uint32_t nbx = ((l.vs >> 1) + SWEEP_BLOCK - 1) / SWEEP_BLOCK;
+    uint32_t nbx = ((l.vs >> 1) + MIN_BLOCK - 1) / MIN_BLOCK;
     size_t need = (size_t)l.nt * nbx * 2 + (size_t)l.nt * 2;
     if (c->part_n < need) {
         cudaFree(c->part);
@@ -524,7 +756,7 @@ struct TrackPtrs {
 };
 static TrackPtrs track_ptrs(gfc_ctx *c) {
     const Lat &l = c->lat;
-    uint32_t nbx = ((l.vs >> 1) + SWEEP_BLOCK - 1) / SWEEP_BLOCK;
+    uint32_t nbx = ((l.vs >> 1) + MIN_BLOCK - 1) / MIN_BLOCK;
     TrackPtrs t;
     t.part = c->part;
     t.slice = c->part + (size_t)l.nt * nbx * 2;
@@ -533,43 +765,129 @@ static TrackPtrs track_ptrs(gfc_ctx *c) {
     return t;
 }
 
+template <class S, int K>
+static void launch_shape(dim3 grid, cudaStream_t st, typename S::V *u, typename S::V *g, const SweepArgs &a) {
+    constexpr int B = kShapes[K].block;
+    grid.x = ((a.l.vs >> 1) + B - 1) / B;
+    k_sweep_fast<S, B, kShapes[K].minb><<<grid, B, 0, st>>>(u, g, a);
+}
+
+template <class S>
+static void dispatch_fast(int v, dim3 grid, cudaStream_t st, typename S::V *u, typename S::V *g,
+                          const SweepArgs &a) {
+    switch (v) {
+        case 0: launch_shape<S, 0>(grid, st, u, g, a); break;
+        case 1: launch_shape<S, 1>(grid, st, u, g, a); break;
+        case 2: launch_shape<S, 2>(grid, st, u, g, a); break;
+        case 3: launch_shape<S, 3>(grid, st, u, g, a); break;
+        case 4: launch_shape<S, 4>(grid, st, u, g, a); break;
+        case 5: launch_shape<S, 5>(grid, st, u, g, a); break;
+        default: launch_shape<S, 6>(grid, st, u, g, a); break;
+    }
+}
+
+// One half-sweep of timeslices [t0, t0 + nsl) (all slices by default).
 template <class S>
 static void launch_fast(gfc_ctx *c, typename S::V *u, typename S::V *g, int sweep, double omega, unsigned hits,
-                        int track, unsigned *stop, double tol_sum) {
+                        int track, unsigned *stop, double tol_sum, int t0 = 0, int nsl = -1) {
     const Lat &l = c->lat;
     TrackPtrs tp = track_ptrs(c);
-    SweepArgs a;
+    SweepArgs a{};
     a.l = l;
     a.par = sweep & 1;
     a.omega = omega;
     a.hits = hits;
     a.track = track;
+    a.t0 = t0;
     a.part = tp.part;
     a.tickets = tp.tickets;
     a.slice = tp.slice;
+    a.ring = c->ring;
+    a.ring_n = c->ring_n;
     a.hist = c->e2_hist;
     a.sweep = sweep;
     a.hist_n = c->hist_n;
     a.stop = stop;
     a.tol_sum = tol_sum;
     a.status = c->dstatus;
-    uint32_t nbx = ((l.vs >> 1) + SWEEP_BLOCK - 1) / SWEEP_BLOCK;
-    k_sweep_fast<S><<<dim3(nbx, l.nt), SWEEP_BLOCK, 0, c->s>>>(u, g, a);
+    const int v = sizeof(typename S::T) == 8 ? c->shape_fast64 : c->shape_fast32;
+    dispatch_fast<S>(v, dim3(0, nsl < 0 ? l.nt : nsl), c->s, u, g, a);
     c->launches++;
 }
 
-void launch_sweep_fast64(gfc_ctx *c, int sweep, double omega, unsigned hits, int track) {
-    if (track && ensure_track_buffers(c, sweep + 1) != GFC_OK) return;
-    if (!c->e2_hist) ensure_track_buffers(c, 1);
-    launch_fast<S64>(c, c->u, c->g, sweep, omega, hits, track, nullptr, 0.0);
-}
-
-template <class S>
-static void launch_reunit(gfc_ctx *c, typename S::V *base, uint32_t nblk, unsigned *stop) {
+// The fast FP64 sweeps keep links and G as two stored rows (1344 B instead of 2016 B
+// of traffic per site-update); the full-matrix fields u, g remain the canonical
+// state that everything else reads.
+static int ensure_2row(gfc_ctx *c) {
     const Lat &l = c->lat;
-    dim3 grid((l.vh + 255) / 256, nblk);
-    k_reunit_fast<S><<<grid, 256, 0, c->s>>>(base, l.vh, nblk, stop, c->dstatus);
+    if (!c->u64r) GFC_CHECK(cudaMalloc(&c->u64r, (size_t)3 * l.npar * l.vh * 6 * sizeof(double2)));
+    if (!c->g64r) GFC_CHECK(cudaMalloc(&c->g64r, (size_t)l.npar * l.vh * 6 * sizeof(double2)));
+    return GFC_OK;
+}
+static void pack_2row(gfc_ctx *c) {
+    const Lat &l = c->lat;
+    dim3 gu((l.vh + 255) / 256, 3 * l.npar), gg((l.vh + 255) / 256, l.npar);
+    k_pack2<<<gu, 256, 0, c->s>>>(c->u, c->u64r, l.vh, 3 * l.npar);
+    k_pack2<<<gg, 256, 0, c->s>>>(c->g, c->g64r, l.vh, l.npar);
+    c->launches += 2;
+}
+static void unpack_2row(gfc_ctx *c) {
+    const Lat &l = c->lat;
+    dim3 gu((l.vh + 255) / 256, 3 * l.npar), gg((l.vh + 255) / 256, l.npar);
+    k_unpack2<<<gu, 256, 0, c->s>>>(c->u64r, c->u, l.vh, 3 * l.npar);
+    k_unpack2<<<gg, 256, 0, c->s>>>(c->g64r, c->g, l.vh, l.npar);
+    c->launches += 2;
+}
+
+int halfsweeps_fast64(gfc_ctx *c, int first, int n, double omega, unsigned hits) {
+    int rc = ensure_track_buffers(c, 1);
+    if (!rc) rc = ensure_2row(c);
+    if (rc) return rc;
+    pack_2row(c);
+    for (int k = 0; k < n; k++) launch_fast<S64R>(c, c->u64r, c->g64r, first + k, omega, hits, 0, nullptr, 0.0);
+    unpack_2row(c);
+    return GFC_OK;
+}
+
+// reunitarise the matrices of timeslices [t0, t0 + nsl) in nblk SoA blocks
+template <class S>
+static void launch_reunit(gfc_ctx *c, typename S::V *base, uint32_t nblk, unsigned *stop, int t0 = 0,
+                          int nsl = -1) {
+    const Lat &l = c->lat;
+    const uint32_t vsh = l.vs >> 1;
+    const uint32_t begin = (uint32_t)t0 * vsh, count = nsl < 0 ? l.vh : (uint32_t)nsl * vsh;
+    dim3 grid((count + 255) / 256, nblk);
+    k_reunit_fast<S><<<grid, 256, 0, c->s>>>(base, l.vh, nblk, begin, count, stop, c->dstatus);
     c->launches++;
+}
+
+static int ensure_ring(gfc_ctx *c, int ring_n) {
+    if (c->ring_n >= ring_n) return GFC_OK;
+    cudaFree(c->ring);
+    c->ring = nullptr;
+    GFC_CHECK(cudaMalloc(&c->ring, (size_t)ring_n * c->lat.nt * 2 * sizeof(double)));
+    c->ring_n = ring_n;
+    return GFC_OK;
+}
+
+// Slice-blocked round: half-sweeps [sweep, kend) applied to one group of G
+// timeslices after another.  Timeslices share no link during the sweeps, so a
+// group can run several half-sweeps while its links and G stay in L2 (kernel
+// boundaries order the half-sweeps); e2 partials go to the per-slice ring.
+template <class S>
+static void sweep_round(gfc_ctx *c, typename S::V *u, typename S::V *g, int sweep, int kend, int G, double omega,
+                        unsigned hits, unsigned reunit, unsigned *stop) {
+    const Lat &l = c->lat;
+    for (int g0 = 0; g0 < l.nt; g0 += G) {
+        const int gn = std::min(G, l.nt - g0);
+        for (int k = sweep; k < kend; k++) {
+            launch_fast<S>(c, u, g, k, omega, hits, 2, stop, 0.0, g0, gn);
+            if (reunit && !((k + 1) % reunit)) {
+                launch_reunit<S>(c, u, 3 * l.npar, stop, g0, gn);
+                launch_reunit<S>(c, g, l.npar, stop, g0, gn);
+            }
+        }
+    }
 }
 
 static void print_res(int sweep, double res) { printf("Sweeps: %8d.\t residue: %3.2E \n", sweep, res); }
@@ -582,47 +900,82 @@ static int initial_proxy(gfc_ctx *c, const gfc_params *p, double *e2, double *re
     return GFC_OK;
 }
 
-// Run fused-e2 half-sweeps of storage S from sweep index `sweep` until the tracked
-// e2 <= tol_e2 (stop word), `max_sweeps` is reached, or an error.  Returns the number
-// of half-sweeps completed in *done (global index), and whether the stop fired.
+static int read_stop(gfc_ctx *c, const unsigned *stop, unsigned *h) {
+    GFC_CHECK(cudaMemcpyAsync(c->hres + 16, stop, sizeof(unsigned), cudaMemcpyDeviceToHost, c->s));
+    GFC_CHECK(cudaStreamSynchronize(c->s));
+    GFC_CHECK(cudaGetLastError());
+    memcpy(h, c->hres + 16, sizeof *h);
+    return GFC_OK;
+}
+
+// Run fused-e2 half-sweeps of storage S from sweep index sweep0 until the tracked
+// e2 <= tol_e2, max_sweeps is reached, or an error.  *done = half-sweeps completed
+// (global index), *first_below = the first half-sweep count whose e2 was seen
+// <= tol (-1 if none).  Unblocked, the kernel that sees it stops the stream (one
+// half-sweep late); slice-blocked, the round in progress is completed.
 template <class S>
 static int run_until(gfc_ctx *c, typename S::V *u, typename S::V *g, int sweep0, int max_sweeps, double tol_e2,
-                     double omega, unsigned hits, unsigned reunit, int *done, int *stopped) {
+                     double omega, unsigned hits, unsigned reunit, int *done, int *first_below) {
     const Lat &l = c->lat;
     int rc = ensure_track_buffers(c, max_sweeps + 2);
     if (rc) return rc;
     TrackPtrs tp = track_ptrs(c);
     GFC_CHECK(cudaMemsetAsync(tp.tickets, 0, (l.nt + 2) * sizeof(unsigned), c->s));
     const double tol_sum = tol_e2 * (double)l.v;
-    const int chunk = 32;
+    const int bs = sizeof(typename S::T) == 8 ? c->blk64_slices : c->blk32_slices;
+    const int bk = sizeof(typename S::T) == 8 ? c->blk64_sweeps : c->blk32_sweeps;
+    const int G = bs > 0 ? std::min(bs, l.nt) : l.nt;
+    const int K = std::max(1, bk);
     int sweep = sweep0;
     unsigned hstop = 0;
-    *stopped = 0;
-    while (sweep < max_sweeps) {
-        int end = std::min(max_sweeps, sweep + chunk);
-        for (; sweep < end; sweep++) {
-            launch_fast<S>(c, u, g, sweep, omega, hits, 1, tp.stop, tol_sum);
-            if (reunit && !((sweep + 1) % reunit)) {
-                launch_reunit<S>(c, u, 3 * l.npar, tp.stop);
-                launch_reunit<S>(c, g, l.npar, tp.stop);
+    *first_below = -1;
+    if (G >= l.nt && K == 1) {
+        const int chunk = 32;
+        while (sweep < max_sweeps) {
+            int end = std::min(max_sweeps, sweep + chunk);
+            for (; sweep < end; sweep++) {
+                launch_fast<S>(c, u, g, sweep, omega, hits, 1, tp.stop, tol_sum);
+                if (reunit && !((sweep + 1) % reunit)) {
+                    launch_reunit<S>(c, u, 3 * l.npar, tp.stop);
+                    launch_reunit<S>(c, g, l.npar, tp.stop);
+                }
             }
+            if ((rc = read_stop(c, tp.stop, &hstop))) return rc;
+            if (hstop) break;
         }
-        GFC_CHECK(cudaMemcpyAsync(c->hres + 16, tp.stop, sizeof(unsigned), cudaMemcpyDeviceToHost, c->s));
-        GFC_CHECK(cudaStreamSynchronize(c->s));
-        GFC_CHECK(cudaGetLastError());
-        memcpy(&hstop, c->hres + 16, sizeof hstop);
+        if (hstop & 0x80000000u) {
+            set_error("NaN in the gauge functional at half-sweep %u", hstop & 0x7fffffffu);
+            return GFC_ERR_NUMERIC;
+        }
+        if (hstop) {
+            *done = (int)hstop;
+            *first_below = (int)hstop - 1;
+        } else {
+            *done = sweep;
+        }
+        return GFC_OK;
+    }
+    if ((rc = ensure_ring(c, K + 2))) return rc;
+    int s_lo = sweep0 + 1;
+    while (sweep < max_sweeps) {
+        const int kend = std::min(max_sweeps, sweep + K);
+        sweep_round<S>(c, u, g, sweep, kend, G, omega, hits, reunit, tp.stop);
+        if (kend - 1 >= s_lo) {
+            k_round_check<<<1, 32, 0, c->s>>>(c->ring, c->ring_n, l.nt, s_lo, kend - 1, c->e2_hist, c->hist_n,
+                                             tol_sum, tp.stop, c->dstatus);
+            c->launches++;
+        }
+        s_lo = kend;
+        sweep = kend;
+        if ((rc = read_stop(c, tp.stop, &hstop))) return rc;
         if (hstop) break;
     }
     if (hstop & 0x80000000u) {
-        set_error("NaN in the gauge functional at half-sweep %u", hstop & 0x7fffffffu);
+        set_error("NaN in the gauge functional at half-sweep %u", hstop & 0x3fffffffu);
         return GFC_ERR_NUMERIC;
     }
-    if (hstop) {
-        *done = (int)hstop;
-        *stopped = 1;
-    } else {
-        *done = sweep;
-    }
+    *done = sweep;
+    if (hstop) *first_below = (int)(hstop & 0x3fffffffu);
     return GFC_OK;
 }
 
@@ -642,15 +995,25 @@ int fix_every_sweep(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_r
     }
     // theta = e2 / 6 identically (gauge_fixing.c:341-442)
     double tol_e2 = p->gfix_proxy == GFC_PROXY_THETA ? 6.0 * p->tolerance : p->tolerance;
-    int done = 0, stopped = 0;
-    rc = run_until<S64>(c, c->u, c->g, 0, (int)p->max_sweeps_to_fix, tol_e2, (double)p->omega_OR, p->hits,
-                        p->sweeps_to_reunitarization, &done, &stopped);
-    if (rc) return rc;
+    int done = 0, below = -1;
+    if (o->precision == GFC_PREC_FP64_FULL) {
+        // plain FP64: full 3x3 storage, same fast arithmetic
+        rc = run_until<S64>(c, c->u, c->g, 0, (int)p->max_sweeps_to_fix, tol_e2, (double)p->omega_OR, p->hits,
+                            p->sweeps_to_reunitarization, &done, &below);
+        if (rc) return rc;
+    } else {
+        if ((rc = ensure_2row(c))) return rc;
+        pack_2row(c);
+        rc = run_until<S64R>(c, c->u64r, c->g64r, 0, (int)p->max_sweeps_to_fix, tol_e2, (double)p->omega_OR,
+                             p->hits, p->sweeps_to_reunitarization, &done, &below);
+        if (rc) return rc;
+        unpack_2row(c);
+    }
     GFC_CHECK(cudaEventRecord(c->ev_d, c->s));
     r->sweeps = done;
-    r->first_below_tol = stopped ? done - 1 : -1;
+    r->first_below_tol = below;
     r->site_updates = (long long)done * l.vh;
-    return stopped ? done : GFC_FIX_NOT_CONVERGED;
+    return below >= 0 ? done : GFC_FIX_NOT_CONVERGED;
 }
 
 int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report *r) {
@@ -684,12 +1047,12 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     }
     // FP32 bulk
     const unsigned reunit32 = std::min<unsigned>(p->sweeps_to_reunitarization, 50u);
-    int done = 0, stopped = 0;
+    int done = 0, below = -1;
     rc = run_until<S32>(c, (float4 *)c->u32, (float4 *)c->g32, 0, (int)p->max_sweeps_to_fix, sw,
-                        (double)p->omega_OR, p->hits, reunit32, &done, &stopped);
+                        (double)p->omega_OR, p->hits, reunit32, &done, &below);
     if (rc) return rc;
     r->sweeps_fp32 = done;
-    if (!stopped) {
+    if (below < 0) {
         r->sweeps = done;
         GFC_CHECK(cudaEventRecord(c->ev_d, c->s));
         return GFC_FIX_NOT_CONVERGED;
@@ -705,15 +1068,216 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     // FP64 refinement
     unsigned reunit64 = o->refine_reunit ? o->refine_reunit : p->sweeps_to_reunitarization;
     int done64 = 0;
-    rc = run_until<S64>(c, c->u, c->g, done, (int)p->max_sweeps_to_fix, tol_e2, (double)p->omega_OR, p->hits,
-                        reunit64, &done64, &stopped);
+    if ((rc = ensure_2row(c))) return rc;
+    pack_2row(c);
+    rc = run_until<S64R>(c, c->u64r, c->g64r, done, (int)p->max_sweeps_to_fix, tol_e2, (double)p->omega_OR,
+                         p->hits, reunit64, &done64, &below);
     if (rc) return rc;
+    unpack_2row(c);
     GFC_CHECK(cudaEventRecord(c->ev_d, c->s));
     r->sweeps = done64;
-    r->first_below_tol = stopped ? done64 - 1 : -1;
+    r->first_below_tol = below;
     // site-updates in each precision
     r->site_updates = (long long)done64 * l.vh;
-    return stopped ? done64 : GFC_FIX_NOT_CONVERGED;
+    return below >= 0 ? done64 : GFC_FIX_NOT_CONVERGED;
 }
 
 }  // namespace gfc
+
+// ------------------------------------------------------------- autotuner --
+// Times every compiled launch shape of the sweep kernels on the resident lattice
+// and keeps the fastest per kernel.  The links are saved first and restored after
+// (the timed half-sweeps change them), and G is reset to the identity.
+// times (optional, length >= GFC_TUNE_SLOTS) receives seconds per half-sweep:
+//   [0..2] exact shapes, [3..9] FP64 fast shapes, [10..16] FP32 shapes (0: not timed).
+using namespace gfc;
+
+extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
+    if (!c) return GFC_ERR_ARG;
+    if (!c->has_links) return GFC_ERR_STATE;
+    if (!which) which = 7;
+    double times[GFC_TUNE_SLOTS] = {0.0};
+    if (times_out)
+        for (int k = 0; k < GFC_TUNE_SLOTS; k++) times_out[k] = 0.0;
+    if (!c->lat.cb) return GFC_OK;   // odd ns: one serial kernel, nothing to choose
+    GFC_CHECK(cudaSetDevice(c->dev));
+    int rc = gfc_ctx_save_links(c);
+    if (rc) return rc;
+    const Lat &l = c->lat;
+    const int n = 6;
+    rc = ensure_track_buffers(c, 2 * n + 2);
+    if (rc) return rc;
+    TrackPtrs tp = track_ptrs(c);
+    cudaEvent_t e0 = c->ev_a, e1 = c->ev_c;
+    auto timed = [&](auto launch) -> double {
+        for (int k = 0; k < 2; k++) launch(k);
+        cudaEventRecord(e0, c->s);
+        for (int k = 0; k < n; k++) launch(k);
+        cudaEventRecord(e1, c->s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms * 1e-3 / n;
+    };
+    auto args_for = [&](int sweep) {
+        SweepArgs a{};
+        a.l = l;
+        a.par = sweep & 1;
+        a.omega = 1.95;
+        a.hits = 2;
+        a.track = 1;
+        a.t0 = 0;
+        a.ring = c->ring;
+        a.ring_n = c->ring_n;
+        a.part = tp.part;
+        a.tickets = tp.tickets;
+        a.slice = tp.slice;
+        a.hist = c->e2_hist;
+        a.sweep = sweep;
+        a.hist_n = c->hist_n;
+        a.stop = nullptr;
+        a.tol_sum = 0.0;
+        a.status = c->dstatus;
+        return a;
+    };
+    if (which & 1) {
+        double best = 1e30;
+        for (int s = 0; s < exact_num_shapes(); s++) {
+            double t = timed([&](int k) { launch_sweep_exact(c->u, c->g, l, k, 1.95, 2, c->s, s); });
+            times[s] = t;
+            if (t < best) {
+                best = t;
+                c->shape_exact = s;
+            }
+        }
+    }
+    if (which & 2) {
+        if ((rc = ensure_2row(c))) return rc;
+        pack_2row(c);
+        double best = 1e30;
+        for (int v = 0; v < kNumShapes; v++) {
+            double t = timed(
+                [&](int k) { dispatch_fast<S64R>(v, dim3(0, l.nt), c->s, c->u64r, c->g64r, args_for(k)); });
+            times[3 + v] = t;
+            if (t < best) {
+                best = t;
+                c->shape_fast64 = v;
+            }
+        }
+    }
+    if ((which & 4) && c->u32 && c->g32) {
+        dim3 gu((l.vh + 255) / 256, 3 * l.npar), gg((l.vh + 255) / 256, l.npar);
+        k_to_f32<<<gu, 256, 0, c->s>>>(c->u, (float4 *)c->u32, l.vh, 3 * l.npar);
+        k_identity32<<<gg, 256, 0, c->s>>>((float4 *)c->g32, l.vh, l.npar);
+        double best = 1e30;
+        for (int v = 0; v < kNumShapes; v++) {
+            double t = timed([&](int k) {
+                dispatch_fast<S32>(v, dim3(0, l.nt), c->s, (float4 *)c->u32, (float4 *)c->g32, args_for(k));
+            });
+            times[10 + v] = t;
+            if (t < best) {
+                best = t;
+                c->shape_fast32 = v;
+            }
+        }
+    }
+    // slice blocking: candidate group sizes from an L2 budget, K half-sweeps per visit
+    GFC_CHECK(cudaMemsetAsync(tp.stop, 0, sizeof(unsigned), c->s));
+    auto tune_blocking = [&](auto tag, auto *u, auto *g, int bytes_per_matrix, int &best_g, int &best_k,
+                             double base_time, double *slot) -> int {
+        using S = decltype(tag);
+        const double slice_bytes = (double)l.vs * 4.0 * bytes_per_matrix;   // 3 links + G per site
+        const int gmax = std::max(1, (int)(96.0e6 / slice_bytes));
+        int cands[3] = {std::max(1, gmax / 2), gmax, 2 * gmax};
+        double best = base_time;
+        best_g = 0;
+        best_k = 1;
+        int slot_i = 0;
+        for (int ci = 0; ci < 3; ci++) {
+            const int G = cands[ci];
+            if (G >= l.nt || (ci > 0 && G == cands[ci - 1])) continue;
+            for (int K : {4, 8}) {
+                int e = ensure_ring(c, K + 2);
+                if (e) return e;
+                sweep_round<S>(c, u, g, 0, K, G, 1.95, 2, 0, tp.stop);   // warm
+                cudaEventRecord(e0, c->s);
+                sweep_round<S>(c, u, g, K, 2 * K, G, 1.95, 2, 0, tp.stop);
+                cudaEventRecord(e1, c->s);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                const double t = ms * 1e-3 / K;
+                if (slot && slot_i < 4) slot[slot_i++] = t;
+                if (t < best) {
+                    best = t;
+                    best_g = G;
+                    best_k = K;
+                }
+            }
+        }
+        return GFC_OK;
+    };
+    if (which & 2) {
+        double base = 1e30;
+        for (int v = 0; v < kNumShapes; v++)
+            if (times[3 + v] > 0 && times[3 + v] < base) base = times[3 + v];
+        rc = tune_blocking(S64R{}, c->u64r, c->g64r, 96, c->blk64_slices, c->blk64_sweeps, base, times + 17);
+        if (rc) return rc;
+    }
+    if ((which & 4) && c->u32 && c->g32) {
+        double base = 1e30;
+        for (int v = 0; v < kNumShapes; v++)
+            if (times[10 + v] > 0 && times[10 + v] < base) base = times[10 + v];
+        rc = tune_blocking(S32{}, (float4 *)c->u32, (float4 *)c->g32, 48, c->blk32_slices, c->blk32_sweeps, base,
+                           times + 21);
+        if (rc) return rc;
+    }
+    GFC_CHECK(cudaGetLastError());
+    rc = gfc_ctx_restore_links(c);
+    if (rc) return rc;
+    launch_identity(c->g, l, c->s);
+    GFC_CHECK(cudaStreamSynchronize(c->s));
+    c->tuned = 1;
+    if (times_out)
+        for (int k = 0; k < GFC_TUNE_SLOTS; k++) times_out[k] = times[k];
+    return GFC_OK;
+}
+
+extern "C" int gfc_ctx_set_blocking(gfc_ctx *c, int precision_bits, int slices, int sweeps) {
+    if (!c || slices < 0 || sweeps < 1) return GFC_ERR_ARG;
+    if (precision_bits & 2) {
+        c->blk64_slices = slices;
+        c->blk64_sweeps = sweeps;
+    }
+    if (precision_bits & 4) {
+        c->blk32_slices = slices;
+        c->blk32_sweeps = sweeps;
+    }
+    return GFC_OK;
+}
+
+extern "C" int gfc_ctx_get_blocking(const gfc_ctx *c, int *s64, int *k64, int *s32, int *k32) {
+    if (!c) return GFC_ERR_ARG;
+    if (s64) *s64 = c->blk64_slices;
+    if (k64) *k64 = c->blk64_sweeps;
+    if (s32) *s32 = c->blk32_slices;
+    if (k32) *k32 = c->blk32_sweeps;
+    return GFC_OK;
+}
+
+extern "C" int gfc_ctx_get_shapes(const gfc_ctx *c, int *exact, int *fast64, int *fast32) {
+    if (!c) return GFC_ERR_ARG;
+    if (exact) *exact = c->shape_exact;
+    if (fast64) *fast64 = c->shape_fast64;
+    if (fast32) *fast32 = c->shape_fast32;
+    return GFC_OK;
+}
+
+extern "C" int gfc_ctx_set_shapes(gfc_ctx *c, int exact, int fast64, int fast32) {
+    if (!c) return GFC_ERR_ARG;
+    if (exact >= exact_num_shapes() || fast64 >= kNumShapes || fast32 >= kNumShapes) return GFC_ERR_ARG;
+    if (exact >= 0) c->shape_exact = exact;
+    if (fast64 >= 0) c->shape_fast64 = fast64;
+    if (fast32 >= 0) c->shape_fast32 = fast32;
+    return GFC_OK;
+}

@@ -4,9 +4,9 @@
 #include "gfc_ctx.h"
 
 namespace gfc {
-// FP64 full-matrix fast half-sweep on the context's u/g; fused e2 partials are
-// written to the context's history when track != 0.
-void launch_sweep_fast64(gfc_ctx *c, int sweep, double omega, unsigned hits, int track);
+// n fast FP64 half-sweeps (indices first..first+n-1) on the context's u/g, run on the
+// two-row working copies (packed before, unpacked after)
+int halfsweeps_fast64(gfc_ctx *c, int first, int n, double omega, unsigned hits);
 // GFC_STOP_EVERY driver (FP64 fast or exact update, proxy tested every half-sweep)
 int fix_every_sweep(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report *r);
 // FP32 two-row bulk until e2 < switch_e2, then FP64 refinement

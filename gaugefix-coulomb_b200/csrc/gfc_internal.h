@@ -14,7 +14,8 @@ namespace gfc {
 
 // ---- exact FP64 kernels (gfc_kernels_exact.cu)
 void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
-                        cudaStream_t s);
+                        cudaStream_t s, int shape = 0);
+int exact_num_shapes();
 void launch_reunitarize(double2 *base, uint32_t stride, uint32_t nblk, unsigned *status, cudaStream_t s);
 void launch_identity(double2 *g, const Lat &l, cudaStream_t s);
 int obs_blocks_per_slice(const Lat &l);

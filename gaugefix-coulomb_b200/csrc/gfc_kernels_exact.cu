@@ -61,9 +61,12 @@ __device__ __forceinline__ void site_update_exact(double2 *__restrict__ u, doubl
     }
 }
 
-__global__ void __launch_bounds__(128) k_sweep_exact(double2 *__restrict__ u, double2 *__restrict__ g, Lat l,
-                                                     int par, double omega, unsigned hits) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+// Launch shapes (threads per block, minimum resident blocks per SM); the second
+// caps registers per thread.  gfc_ctx_autotune picks one per lattice.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_sweep_exact(double2 *__restrict__ u, double2 *__restrict__ g,
+                                                             Lat l, int par, double omega, unsigned hits) {
+    uint32_t i = blockIdx.x * BLOCK + threadIdx.x;
     if (i >= l.vh) return;
     Coord c = coord_cb(l, par, i);
     site_update_exact<true>(u, g, l, par, c, omega, hits);
@@ -83,12 +86,23 @@ __global__ void k_sweep_exact_serial(double2 *__restrict__ u, double2 *__restric
     }
 }
 
+int exact_num_shapes() { return 3; }
+
 void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
-                        cudaStream_t s) {
+                        cudaStream_t s, int shape) {
     if (l.cb) {
         int par = sweep & 1;  // BLACKRED_SWEEP: even sites on even sweeps (gauge_fixing.c:42)
-        unsigned blocks = (l.vh + 127) / 128;
-        k_sweep_exact<<<blocks, 128, 0, s>>>(u, g, l, par, omega, hits);
+        switch (shape) {
+            case 1:
+                k_sweep_exact<128, 3><<<(l.vh + 127) / 128, 128, 0, s>>>(u, g, l, par, omega, hits);
+                break;
+            case 2:
+                k_sweep_exact<64, 4><<<(l.vh + 63) / 64, 64, 0, s>>>(u, g, l, par, omega, hits);
+                break;
+            default:
+                k_sweep_exact<128, 1><<<(l.vh + 127) / 128, 128, 0, s>>>(u, g, l, par, omega, hits);
+                break;
+        }
     } else {
         unsigned blocks = (l.nt + 31) / 32;
         k_sweep_exact_serial<<<blocks, 32, 0, s>>>(u, g, l, sweep, omega, hits);

@@ -23,7 +23,7 @@ GFC_OK = 0
 FIX_NOT_CONVERGED = -1
 FIX_BAD_PARAMS = -2
 PROXY_E2, PROXY_THETA = 0, 1
-PREC_FP64_EXACT, PREC_FP64_FAST, PREC_MIXED = 0, 1, 2
+PREC_FP64_EXACT, PREC_FP64_FAST, PREC_MIXED, PREC_FP64_FULL = 0, 1, 2, 3
 STOP_REFERENCE, STOP_EVERY = 0, 1
 CTX_MIXED = 1
 
@@ -122,6 +122,11 @@ def _load():
         "gfc_ctx_finalize_temporal": (I, [P]),
         "gfc_ctx_fix": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), ctypes.POINTER(Report)]),
         "gfc_e2_theta_device_noalloc": (I, [I, I, P, P, DP, DP]),
+        "gfc_ctx_autotune": (I, [P, I, P]),
+        "gfc_ctx_get_shapes": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "gfc_ctx_set_shapes": (I, [P, I, I, I]),
+        "gfc_ctx_set_blocking": (I, [P, I, I, I]),
+        "gfc_ctx_get_blocking": (I, [P] + [ctypes.POINTER(I)] * 4),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -275,6 +280,30 @@ class Lattice:
 
     def sync(self):
         _check(lib.gfc_ctx_sync(self.h), "sync")
+
+    def autotune(self, which=0):
+        """Time every compiled launch shape on this lattice; keep the fastest.
+        Returns seconds per half-sweep: {"exact": [...], "fast64": [...], "fast32": [...]}."""
+        t = np.zeros(25)
+        _check(lib.gfc_ctx_autotune(self.h, which, t.ctypes.data), "autotune")
+        return {"exact": t[0:3].tolist(), "fast64": t[3:10].tolist(), "fast32": t[10:17].tolist(),
+                "fast64_blocked": t[17:21].tolist(), "fast32_blocked": t[21:25].tolist()}
+
+    def set_blocking(self, precision_bits, slices, sweeps):
+        _check(lib.gfc_ctx_set_blocking(self.h, precision_bits, slices, sweeps), "set_blocking")
+
+    def blocking(self):
+        v = [ctypes.c_int() for _ in range(4)]
+        _check(lib.gfc_ctx_get_blocking(self.h, *[ctypes.byref(x) for x in v]), "get_blocking")
+        return tuple(x.value for x in v)
+
+    def shapes(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib.gfc_ctx_get_shapes(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "get_shapes")
+        return a.value, b.value, c.value
+
+    def set_shapes(self, exact=-1, fast64=-1, fast32=-1):
+        _check(lib.gfc_ctx_set_shapes(self.h, exact, fast64, fast32), "set_shapes")
 
     @property
     def kernel_launches(self):

@@ -72,8 +72,9 @@ void gfc_params_print(const gfc_params *p);
 /* ---- run options (no counterpart in the reference: GPU execution choices) ---- */
 typedef enum {
     GFC_PREC_FP64_EXACT = 0, /* FP64, reference arithmetic: bit-for-bit the reference update */
-    GFC_PREC_FP64_FAST  = 1, /* FP64, direct SU(2) accumulation, FMA                       */
-    GFC_PREC_MIXED      = 2  /* FP32 bulk sweeps, FP64 refinement                           */
+    GFC_PREC_FP64_FAST  = 1, /* FP64, direct SU(2) accumulation, FMA, two stored rows per matrix */
+    GFC_PREC_MIXED      = 2, /* FP32 bulk sweeps (two rows), FP64 two-row refinement          */
+    GFC_PREC_FP64_FULL  = 3  /* FP64 fast arithmetic on full 3x3 storage (plain FP64)          */
 } gfc_precision;
 
 typedef enum {
@@ -181,6 +182,27 @@ int  gfc_ctx_plaquette(gfc_ctx *c, double *spatial, double *temporal);
 int  gfc_ctx_halfsweeps(gfc_ctx *c, int first_sweep, int n, float omega_OR, unsigned hits, int precision);
 /* apply G to the temporal links (U_t(x) <- G(x) U_t(x) G(x+t)^dagger) and reunitarise them */
 int  gfc_ctx_finalize_temporal(gfc_ctx *c);
+
+/* ---- launch-shape autotuner (no counterpart in the reference) ------------------------ */
+/* Times every compiled launch shape (threads per block x resident blocks per SM)
+ * of the sweep kernels on this lattice and keeps the fastest for later fixes.
+ * which: bit 0 exact FP64, bit 1 fast FP64, bit 2 FP32 (0 = all).  The links are
+ * saved and restored around the timing (a device copy of all links is kept) and G
+ * is reset to the identity.  times (may be NULL) receives seconds per half-sweep:
+ * [0..2] exact shapes, [3..9] fast FP64 shapes, [10..16] FP32 shapes, [17..20] fast
+ * FP64 slice-blocked candidates, [21..24] FP32 slice-blocked candidates.  Slice
+ * blocking runs a group of timeslices for several half-sweeps while its links stay in
+ * L2 (timeslices share no link during the sweeps); it is kept only where it measured
+ * faster. */
+#define GFC_TUNE_SLOTS 25
+int  gfc_ctx_autotune(gfc_ctx *c, int which, double *times);
+int  gfc_ctx_get_shapes(const gfc_ctx *c, int *exact, int *fast64, int *fast32);
+/* -1 keeps the current choice */
+int  gfc_ctx_set_shapes(gfc_ctx *c, int exact, int fast64, int fast32);
+/* slice blocking for the fast FP64 (bit 1) and/or FP32 (bit 2) sweeps: groups of
+ * `slices` timeslices, `sweeps` half-sweeps per visit (0 / 1: no blocking) */
+int  gfc_ctx_set_blocking(gfc_ctx *c, int precision_bits, int slices, int sweeps);
+int  gfc_ctx_get_blocking(const gfc_ctx *c, int *slices64, int *sweeps64, int *slices32, int *sweeps32);
 
 /* ---- allocation-free observable --------------------------------------------------- */
 /* e2 and theta (the quantities of gfc_ctx_e2) of links the caller already holds in

@@ -84,3 +84,61 @@ def test_fast_tracks_exact_per_sweep():
             out[prec] = (np.array(e2), lat.functional())
     np.testing.assert_allclose(out[gfc.PREC_FP64_FAST][0], out[gfc.PREC_FP64_EXACT][0], rtol=1e-6)
     assert out[gfc.PREC_FP64_FAST][1] == pytest.approx(out[gfc.PREC_FP64_EXACT][1], rel=1e-12)
+
+
+def test_every_launch_shape_gives_identical_results():
+    """The autotuner may pick any compiled shape: all of them compute the same bits."""
+    ns, nt = 8, 8
+    U0 = gfc.synth_config(ns, nt, 53, 0.5)
+    orc.reunitarize(U0)
+    results = {}
+    with gfc.Lattice(ns, nt, mixed=True) as lat:
+        lat.upload_links(U0, 8, False)
+        lat.save_links()
+        times = lat.autotune()
+        assert all(t > 0 for t in times["exact"] + times["fast64"] + times["fast32"])
+        assert lat.download_links().tobytes() == U0.tobytes()   # restored after tuning
+        for kind, n in (("exact", 3), ("fast64", 7), ("fast32", 7)):
+            outs = set()
+            for s in range(n):
+                lat.restore_links()
+                lat.set_shapes(**{kind: s})
+                prec = {"exact": gfc.PREC_FP64_EXACT, "fast64": gfc.PREC_FP64_FAST, "fast32": gfc.PREC_MIXED}[kind]
+                rc, rep = lat.fix(gfc.default_params(tolerance=1e-14),
+                                  gfc.options(precision=prec, stop_rule=gfc.STOP_EVERY))
+                assert rc > 0
+                outs.add(orc.sha(lat.download_gt()))
+            results[kind] = outs
+    for kind, outs in results.items():
+        assert len(outs) == 1, kind
+
+
+def test_slice_blocking_same_results():
+    """Timeslices share no link during the sweeps, so running groups of them for
+    several half-sweeps at a time changes nothing but the order of independent
+    work: same first half-sweep below tolerance, and G bit-identical to the same
+    number of unblocked half-sweeps."""
+    ns, nt = 8, 8
+    U0 = gfc.synth_config(ns, nt, 54, 0.5)
+    orc.reunitarize(U0)
+    p = gfc.default_params(tolerance=1e-15, sweeps_to_reunitarization=100000)
+    o = gfc.options(precision=gfc.PREC_FP64_FAST, stop_rule=gfc.STOP_EVERY)
+    with gfc.Lattice(ns, nt, mixed=True) as lat:
+        lat.upload_links(U0, 8, False)
+        lat.save_links()
+        rc0, r0 = lat.fix(p, o)
+        lat.restore_links()
+        lat.set_blocking(2 | 4, 3, 4)          # groups of 3 slices (ragged last group), 4 half-sweeps
+        rc1, r1 = lat.fix(p, o)
+        G1 = lat.download_gt()
+        assert r1.first_below_tol == r0.first_below_tol
+        assert rc1 % 4 == 0 and rc1 >= r0.first_below_tol + 1 and r1.final_residue <= 1e-15
+        lat.restore_links()
+        lat.set_identity_gt()
+        lat.halfsweeps(0, rc1, 1.95, 2, gfc.PREC_FP64_FAST)
+        lat.reunitarize_gt()
+        assert orc.sha(lat.download_gt()) == orc.sha(G1)
+        # mixed precision with blocking in both phases still reaches the tolerance
+        lat.restore_links()
+        rc2, r2 = lat.fix(p, gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY))
+        assert rc2 > 0 and r2.final_residue <= 1e-15
