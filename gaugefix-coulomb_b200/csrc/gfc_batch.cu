@@ -1,0 +1,959 @@
+// gfc_batch.cu -- many lattices at once, with per-timeslice retirement.
+//
+// The Coulomb gauge condition decouples timeslices: during the sweeps a timeslice
+// shares no link with another.  The batch therefore schedules timeslices, not
+// lattices.  Every timeslice of every resident lattice ("slot") carries a state:
+//
+//   FP32   bulk sweeps on two-row FP32 links and G
+//   PEND   its FP32 e2 fell below the switch threshold: rebuild in FP64 next round
+//   FP64   refinement on two-row FP64 links and G
+//   DONE   its own e2 fell below the tolerance: retired, no more work
+//
+// A round is: compaction (work lists of (timeslice, 128-site chunk) items for the
+// FP32 and FP64 states and of pending timeslices), the FP64 rebuild of the pending
+// timeslices (G from its FP32 copy, projected; links as G U0 G^dagger from the FP64
+// originals), then K half-sweeps, each one persistent FP32 kernel and one
+// persistent FP64 kernel over their work lists, plus periodic reunitarisation.
+// All parameters live in device memory, so one round is captured once as a CUDA
+// graph and replayed; the host only reads the state table between rounds.
+//
+// Inside a sweep kernel the last chunk of a timeslice to finish (ticket counter)
+// sums the chunk partials of the fused e2 in chunk order, adds the other parity's
+// contribution from the previous half-sweep (ring buffer) and decides the switch or
+// the retirement of that timeslice alone.
+//
+// Slots can be added, activated, finalised and removed between rounds, which is
+// what the serving loop does (continuous batching).
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gfc.h"
+#include "gfc_ctx.h"
+#include "gfc_fast_device.cuh"
+#include "gfc_internal.h"
+
+namespace gfc {
+
+enum : int { SS_EMPTY = 0, SS_FP32 = 1, SS_PEND = 2, SS_FP64 = 3, SS_DONE = 4 };
+constexpr int BCHUNK = 128;   // sites per work item = threads per CTA of the sweep kernels
+
+struct BSlot {          // device-visible descriptor of one resident lattice
+    Lat l;
+    double2 *u, *ut, *g;   // FP64 full: canonical links and G
+    double2 *u64r, *g64r;  // FP64 two-row working copies
+    float4 *u32, *g32;     // FP32 two-row working copies
+    double *part;          // [nt][nbx][2] chunk partials of the fused e2
+    unsigned *tickets;     // [nt]
+    int nbx;               // chunks per timeslice and parity = ceil(vs/2 / BCHUNK)
+    int nfull;             // chunks per timeslice over both parities = ceil(vs / BCHUNK)
+};
+
+struct BState {
+    BSlot *slots;
+    int max_nt, nslices;
+    int *state;           // [nslices], gid = slot * max_nt + t
+    int *sweeps;          // [nslices] half-sweeps applied to the timeslice
+    double *ring;         // [2][nslices][2]: (pre, post) e2 sums of the last two half-sweeps
+    int2 *items32, *items64, *pend;
+    int cap_items, cap_pend;
+    int *counts;          // [0] n32 [1] n64 [2] npend [3] active timeslices [4] half-sweep k [5] overflow
+    unsigned *status;
+    double omega, switch_e2, tol;
+    unsigned hits, reunit32, reunit64;
+};
+
+// ------------------------------------------------------------------ compaction --
+// One block.  Builds the three work lists from the state table.
+__global__ void __launch_bounds__(1024) k_compact(BState b) {
+    __shared__ int sc[3][1024];
+    __shared__ int sact[1024];
+    const int tid = threadIdx.x;
+    const int per = (b.nslices + 1023) / 1024;
+    const int g0 = tid * per, g1 = min(g0 + per, b.nslices);
+    int c[3] = {0, 0, 0}, act = 0;
+    for (int gid = g0; gid < g1; gid++) {
+        int st = b.state[gid];
+        if (st == SS_EMPTY || st == SS_DONE) continue;
+        const BSlot &sl = b.slots[gid / b.max_nt];
+        act++;
+        if (st == SS_FP32) c[0] += sl.nbx;
+        else if (st == SS_FP64) c[1] += sl.nbx;
+        else if (st == SS_PEND) c[2] += sl.nfull;
+    }
+    for (int q = 0; q < 3; q++) sc[q][tid] = c[q];
+    sact[tid] = act;
+    __syncthreads();
+    // inclusive Hillis-Steele scans
+    for (int off = 1; off < 1024; off <<= 1) {
+        int v[3], a = 0;
+        for (int q = 0; q < 3; q++) v[q] = tid >= off ? sc[q][tid - off] : 0;
+        if (tid >= off) a = sact[tid - off];
+        __syncthreads();
+        for (int q = 0; q < 3; q++) sc[q][tid] += v[q];
+        sact[tid] += a;
+        __syncthreads();
+    }
+    int o[3];
+    for (int q = 0; q < 3; q++) o[q] = sc[q][tid] - c[q];
+    int overflow = 0;
+    for (int gid = g0; gid < g1; gid++) {
+        int st = b.state[gid];
+        if (st == SS_EMPTY || st == SS_DONE) continue;
+        const BSlot &sl = b.slots[gid / b.max_nt];
+        if (st == SS_FP32 || st == SS_FP64) {
+            int q = st == SS_FP32 ? 0 : 1;
+            int2 *lst = q == 0 ? b.items32 : b.items64;
+            for (int ch = 0; ch < sl.nbx; ch++, o[q]++)
+                if (o[q] < b.cap_items) lst[o[q]] = make_int2(gid, ch);
+                else overflow = 1;
+        } else if (st == SS_PEND) {
+            for (int ch = 0; ch < sl.nfull; ch++, o[2]++)
+                if (o[2] < b.cap_pend) b.pend[o[2]] = make_int2(gid, ch);
+                else overflow = 1;
+        }
+    }
+    if (overflow) atomicOr(&b.counts[5], 1);
+    if (tid == 1023) {
+        b.counts[0] = min(sc[0][1023], b.cap_items);
+        b.counts[1] = min(sc[1][1023], b.cap_items);
+        b.counts[2] = min(sc[2][1023], b.cap_pend);
+        b.counts[3] = sact[1023];
+    }
+}
+
+// ---------------------------------------------------------- the sweep kernels --
+template <class S>
+__device__ __forceinline__ void slot_fields(const BSlot &sl, typename S::V *&u, typename S::V *&g) {
+    if constexpr (sizeof(typename S::T) == 8) {
+        u = sl.u64r;
+        g = sl.g64r;
+    } else {
+        u = sl.u32;
+        g = sl.g32;
+    }
+}
+
+template <class S, int MINB>
+__global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
+    using T = typename S::T;
+    using C = typename CT<T>::t;
+    constexpr bool F64 = sizeof(T) == 8;
+    __shared__ double sh[2][BCHUNK / 32];
+    __shared__ int last;
+    const int n = b.counts[F64 ? 1 : 0];
+    const int k = b.counts[4];
+    const int par = k & 1, op = par ^ 1;
+    const int expect = F64 ? SS_FP64 : SS_FP32;
+    const int2 *items = F64 ? b.items64 : b.items32;
+    for (int it = blockIdx.x; it < n; it += gridDim.x) {
+        const int2 item = items[it];
+        const int gid = item.x, chunk = item.y;
+        if (*(volatile int *)&b.state[gid] != expect) continue;   // the same for every thread of the CTA
+        const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
+        const BSlot &sl = b.slots[slot];
+        const Lat l = sl.l;
+        typename S::V *u, *g;
+        slot_fields<S>(sl, u, g);
+        const uint32_t vsh = l.vs >> 1;
+        const uint32_t off = (uint32_t)chunk * BCHUNK + threadIdx.x;
+        double pre = 0.0, post = 0.0;
+        if (off < vsh) {
+            const uint32_t i = (uint32_t)t * vsh + off;
+            Coord c = coord_cb(l, par, i);
+            uint32_t ib[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) ib[d] = back_L(l, c, d) >> 1;
+            Mt<T> w;
+#pragma unroll
+            for (int q = 0; q < 9; q++) w.e[q] = mkc<C>(T(0), T(0));
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                Mt<T> f, r;
+                S::load(u + su_idx<S>(l, d, par, i), l.vh, f);
+                S::load(u + su_idx<S>(l, d, op, ib[d]), l.vh, r);
+#pragma unroll
+                for (int x = 0; x < 3; x++)
+#pragma unroll
+                    for (int y = 0; y < 3; y++)
+                        w.e[EL(x, y)] = fadd(w.e[EL(x, y)], fadd(f.e[EL(x, y)], fconj(r.e[EL(y, x)])));
+            }
+            pre = e2_from_w(w);
+            Mt<T> up;
+            fupdate(w, (T)b.omega, b.hits, up);
+            {
+                Mt<T> m, o;
+                S::load(g + sg_idx<S>(l, par, i), l.vh, m);
+                fprod_left<S>(up, m, o);
+                S::store(g + sg_idx<S>(l, par, i), l.vh, o);
+            }
+            double cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                apply_forward<S>(u + su_idx<S>(l, d, par, i), l.vh, up, 1, cc);
+                apply_backward<S>(u + su_idx<S>(l, d, op, ib[d]), l.vh, up, 1, cc);
+            }
+            cc[7] *= 0.57735026918962576451;
+#pragma unroll
+            for (int q = 0; q < 8; q++) post += cc[q] * cc[q];
+        }
+        // chunk partials (deterministic order inside the block)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            pre += __shfl_down_sync(0xffffffffu, pre, o);
+            post += __shfl_down_sync(0xffffffffu, post, o);
+        }
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) {
+            sh[0][wid] = pre;
+            sh[1][wid] = post;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s0 = 0.0, s1 = 0.0;
+            for (int q = 0; q < BCHUNK / 32; q++) {
+                s0 += sh[0][q];
+                s1 += sh[1][q];
+            }
+            double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
+            pp[0] = s0;
+            pp[1] = s1;
+            __threadfence();
+            last = atomicAdd(&sl.tickets[t], 1u) == (unsigned)sl.nbx - 1;
+        }
+        __syncthreads();
+        if (last && threadIdx.x == 0) {
+            double s0 = 0.0, s1 = 0.0;
+            const double *pp = sl.part + (size_t)t * sl.nbx * 2;
+            for (int q = 0; q < sl.nbx; q++) {
+                s0 += __ldcg(pp + 2 * q);
+                s1 += __ldcg(pp + 2 * q + 1);
+            }
+            sl.tickets[t] = 0;
+            double *rprev = b.ring + ((size_t)((k + 1) & 1) * b.nslices + gid) * 2;
+            double *rcur = b.ring + ((size_t)(k & 1) * b.nslices + gid) * 2;
+            const double e2s = (s0 + __ldcg(rprev + 1)) / (double)l.vs;   // e2 of the timeslice after k half-sweeps
+            rcur[0] = s0;
+            rcur[1] = s1;
+            b.sweeps[gid] += 1;
+            if (!(s0 == s0) || !(s1 == s1)) {
+                atomicOr(b.status, GFC_STATUS_NAN);
+                b.state[gid] = SS_DONE;
+            } else if (!F64 && e2s <= b.switch_e2) {
+                b.state[gid] = SS_PEND;
+            } else if (F64 && e2s <= b.tol) {
+                b.state[gid] = SS_DONE;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_btick(BState b) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) b.counts[4] += 1;
+}
+
+// projectSU3 of a timeslice's working fields after every `period` of its own
+// half-sweeps (its own count, so a lattice admitted later is treated exactly as if
+// it were alone)
+template <class S>
+__global__ void __launch_bounds__(BCHUNK) k_breunit(BState b, unsigned period) {
+    constexpr bool F64 = sizeof(typename S::T) == 8;
+    if (period == 0) return;
+    const int n = b.counts[F64 ? 1 : 0];
+    const int2 *items = F64 ? b.items64 : b.items32;
+    const int expect = F64 ? SS_FP64 : SS_FP32;
+    for (int it = blockIdx.x; it < n; it += gridDim.x) {
+        const int2 item = items[it];
+        const int gid = item.x;
+        if (*(volatile int *)&b.state[gid] != expect) continue;
+        const int own = b.sweeps[gid];
+        if (own == 0 || (unsigned)own % period) continue;
+        const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
+        const BSlot &sl = b.slots[slot];
+        const Lat l = sl.l;
+        typename S::V *u, *g;
+        slot_fields<S>(sl, u, g);
+        const uint32_t vsh = l.vs >> 1;
+        const uint32_t off = (uint32_t)item.y * BCHUNK + threadIdx.x;
+        if (off >= vsh) continue;
+        const uint32_t i = (uint32_t)t * vsh + off;
+        for (int par = 0; par < 2; par++) {
+            for (int d = 0; d <= 3; d++) {
+                typename S::V *p = d < 3 ? u + su_idx<S>(l, d, par, i) : g + sg_idx<S>(l, par, i);
+                Mt<typename S::T> m;
+                S::load(p, l.vh, m);
+                if (!fproject(m)) atomicOr(b.status, GFC_STATUS_PROJECT_FAIL);
+                S::store(p, l.vh, m);
+            }
+        }
+    }
+}
+
+// --------------------------------------------------- FP32 -> FP64 switch --
+// pass 1: G in FP64 (row 2 rebuilt from the FP32 rows, projected) into g and g64r
+__global__ void __launch_bounds__(BCHUNK) k_switch_g(BState b) {
+    const int n = b.counts[2];
+    for (int it = blockIdx.x; it < n; it += gridDim.x) {
+        const int2 item = b.pend[it];
+        const int slot = item.x / b.max_nt, t = item.x - slot * b.max_nt;
+        const BSlot &sl = b.slots[slot];
+        const Lat l = sl.l;
+        const uint32_t r = (uint32_t)item.y * BCHUNK + threadIdx.x;
+        if (r >= l.vs) continue;
+        const Slot s = slot_of(l, (uint32_t)t * l.vs + r);
+        Mt<float> m32;
+        S32::load_rows01(sl.g32 + sg_idx<S32>(l, s.par, s.i), l.vh, m32);
+        Mt<double> m;
+        for (int q = 0; q < 6; q++) m.e[q] = make_double2(m32.e[q].x, m32.e[q].y);
+        if (!fproject(m)) fidentity(m);
+        S64::store(sl.g + sg_idx<S64>(l, s.par, s.i), l.vh, m);
+        S64R::store(sl.g64r + sg_idx<S64R>(l, s.par, s.i), l.vh, m);
+    }
+}
+
+// pass 2: links U_d(x) = G(x) U0_d(x) G(x+d)^dagger from the FP64 originals into u64r
+__global__ void __launch_bounds__(BCHUNK) k_switch_u(BState b) {
+    const int n = b.counts[2];
+    for (int it = blockIdx.x; it < n; it += gridDim.x) {
+        const int2 item = b.pend[it];
+        const int slot = item.x / b.max_nt, t = item.x - slot * b.max_nt;
+        const BSlot &sl = b.slots[slot];
+        const Lat l = sl.l;
+        const uint32_t r = (uint32_t)item.y * BCHUNK + threadIdx.x;
+        if (r >= l.vs) continue;
+        const uint32_t L = (uint32_t)t * l.vs + r;
+        const Coord c = coord_lex(l, L);
+        const Slot s = slot_of(l, L);
+        M3 gx;
+        load_m(sl.g + gidx(l, s.par, 0, s.i), l.vh, gx);
+        for (int d = 0; d < 3; d++) {
+            const Slot sy = slot_of(l, fwd_L(l, c, d));
+            M3 gy, u0, tmp, o;
+            load_m(sl.g + gidx(l, sy.par, 0, sy.i), l.vh, gy);
+            load_m(sl.u + uidx(l, d, s.par, 0, s.i), l.vh, u0);
+            xprod(gx, u0, tmp);
+            xprod_dag(tmp, gy, o);
+            double2 *q = sl.u64r + su_idx<S64R>(l, d, s.par, s.i);
+#pragma unroll
+            for (int e = 0; e < 6; e++) q[(size_t)e * l.vh] = o.e[e];
+        }
+    }
+}
+
+// pass 3: pending timeslices become FP64; the previous e2 entry is invalidated
+__global__ void k_switch_done(BState b) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= b.nslices || b.state[gid] != SS_PEND) return;
+    b.state[gid] = SS_FP64;
+    b.ring[((size_t)0 * b.nslices + gid) * 2 + 1] = __longlong_as_double(0x7ff0000000000000LL);
+    b.ring[((size_t)1 * b.nslices + gid) * 2 + 1] = __longlong_as_double(0x7ff0000000000000LL);
+}
+
+// activate the timeslices of one slot in `state`
+__global__ void k_activate(BState b, int gid0, int nt, int state) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    const int gid = gid0 + t;
+    b.state[gid] = state;
+    b.sweeps[gid] = 0;
+    for (int q = 0; q < 2; q++) {
+        b.ring[((size_t)q * b.nslices + gid) * 2] = 0.0;
+        b.ring[((size_t)q * b.nslices + gid) * 2 + 1] = __longlong_as_double(0x7ff0000000000000LL);
+    }
+}
+
+__global__ void k_set_state(int *state, int gid0, int nt, int value) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nt) state[gid0 + t] = value;
+}
+
+}  // namespace gfc
+
+using namespace gfc;
+
+// ================================================================== host ==
+struct gfc_batch {
+    int dev = 0;
+    cudaStream_t s = nullptr;
+    int max_slots = 0, max_nt = 0, nslices = 0;
+    size_t max_sites = 0, used_sites = 0;
+    std::vector<BSlot> hs;          // host copies of the descriptors
+    std::vector<void *> mem;        // per-slot allocation
+    std::vector<int> used, ns, nt, activated;
+    BSlot *dslots = nullptr;
+    int *state = nullptr, *sweeps = nullptr, *counts = nullptr;
+    double *ring = nullptr;
+    int2 *items32 = nullptr, *items64 = nullptr, *pend = nullptr;
+    int cap_items = 0, cap_pend = 0;
+    unsigned *status = nullptr;
+    int *hcounts = nullptr;          // pinned mirror [8]
+    int *hstate = nullptr;           // pinned mirror [nslices]
+    // observables scratch (sized for the largest slot)
+    double *part = nullptr, *dres = nullptr, *hres = nullptr;
+    size_t part_n = 0;
+    // the captured round
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int round_k = 8;
+    BState captured{};
+    int grid = 0;
+    int minb32 = 4, minb64 = 3;
+    long long launches = 0;
+    long long rounds = 0;
+};
+
+static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+extern "C" int gfc_batch_create(int device, size_t max_sites, int max_slots, int max_nt, gfc_batch **out) {
+    if (!out || max_slots <= 0 || max_nt <= 0 || max_sites == 0) return GFC_ERR_ARG;
+    *out = nullptr;
+    gfc_batch *b = new gfc_batch();
+    b->dev = device;
+    b->max_slots = max_slots;
+    b->max_nt = max_nt;
+    b->nslices = max_slots * max_nt;
+    b->max_sites = max_sites;
+    b->hs.assign(max_slots, BSlot{});
+    b->mem.assign(max_slots, nullptr);
+    b->used.assign(max_slots, 0);
+    b->ns.assign(max_slots, 0);
+    b->nt.assign(max_slots, 0);
+    b->activated.assign(max_slots, 0);
+    // work lists: every chunk of every timeslice (upper bound)
+    b->cap_items = (int)(max_sites / 2 / BCHUNK + (size_t)b->nslices + 1024);
+    b->cap_pend = (int)(max_sites / BCHUNK + (size_t)b->nslices + 1024);
+    int rc = GFC_OK;
+    cudaError_t e;
+#define BTRY(call)                          \
+    if ((e = (call)) != cudaSuccess) {      \
+        rc = cuda_fail(e, #call);           \
+        goto fail;                          \
+    }
+    BTRY(cudaSetDevice(device));
+    BTRY(cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking));
+    BTRY(cudaMalloc(&b->dslots, sizeof(BSlot) * max_slots));
+    BTRY(cudaMemset(b->dslots, 0, sizeof(BSlot) * max_slots));
+    BTRY(cudaMalloc(&b->state, sizeof(int) * b->nslices));
+    BTRY(cudaMemset(b->state, 0, sizeof(int) * b->nslices));
+    BTRY(cudaMalloc(&b->sweeps, sizeof(int) * b->nslices));
+    BTRY(cudaMemset(b->sweeps, 0, sizeof(int) * b->nslices));
+    BTRY(cudaMalloc(&b->ring, sizeof(double) * 4 * b->nslices));
+    BTRY(cudaMalloc(&b->items32, sizeof(int2) * b->cap_items));
+    BTRY(cudaMalloc(&b->items64, sizeof(int2) * b->cap_items));
+    BTRY(cudaMalloc(&b->pend, sizeof(int2) * b->cap_pend));
+    BTRY(cudaMalloc(&b->counts, sizeof(int) * 8));
+    BTRY(cudaMemset(b->counts, 0, sizeof(int) * 8));
+    BTRY(cudaMalloc(&b->status, sizeof(unsigned)));
+    BTRY(cudaMemset(b->status, 0, sizeof(unsigned)));
+    BTRY(cudaMallocHost(&b->hcounts, sizeof(int) * 8));
+    BTRY(cudaMallocHost(&b->hstate, sizeof(int) * b->nslices));
+    BTRY(cudaMalloc(&b->dres, sizeof(double) * 8));
+    BTRY(cudaMallocHost(&b->hres, sizeof(double) * 8));
+    {
+        int nsm = 0;
+        BTRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+        b->grid = nsm * 4;   // persistent CTAs; more than resident is harmless (they loop)
+    }
+#undef BTRY
+    *out = b;
+    return GFC_OK;
+fail:
+    delete b;
+    return rc;
+}
+
+extern "C" int gfc_batch_destroy(gfc_batch *b) {
+    if (!b) return GFC_ERR_ARG;
+    cudaSetDevice(b->dev);
+    cudaStreamSynchronize(b->s);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (void *m : b->mem)
+        if (m) cudaFree(m);
+    cudaFree(b->dslots);
+    cudaFree(b->state);
+    cudaFree(b->sweeps);
+    cudaFree(b->ring);
+    cudaFree(b->items32);
+    cudaFree(b->items64);
+    cudaFree(b->pend);
+    cudaFree(b->counts);
+    cudaFree(b->status);
+    cudaFree(b->part);
+    cudaFree(b->dres);
+    cudaFreeHost(b->hcounts);
+    cudaFreeHost(b->hstate);
+    cudaFreeHost(b->hres);
+    if (b->s) cudaStreamDestroy(b->s);
+    delete b;
+    return GFC_OK;
+}
+
+// bytes of device memory one slot of ns^3 x nt needs
+extern "C" size_t gfc_batch_slot_bytes(int ns, int nt) {
+    Lat l = make_lat(ns, nt);
+    size_t vh = l.vh;
+    size_t nbx = ((l.vs >> 1) + BCHUNK - 1) / BCHUNK;
+    return al256(3 * 2 * vh * 9 * 16) + 2 * al256(2 * vh * 9 * 16)            // u, ut, g
+           + al256(3 * 2 * vh * 6 * 16) + al256(2 * vh * 6 * 16)              // u64r, g64r
+           + al256(3 * 2 * vh * 3 * 16) + al256(2 * vh * 3 * 16)              // u32, g32
+           + al256((size_t)nt * nbx * 2 * 8) + al256((size_t)nt * 4) + 4096;  // part, tickets
+}
+
+extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
+    if (!b || !slot_out) return GFC_ERR_ARG;
+    *slot_out = -1;
+    if (ns <= 0 || nt <= 0 || (ns & 1) || nt > b->max_nt) {
+        set_error("batch slots need even ns and nt <= %d (got %d, %d)", b->max_nt, ns, nt);
+        return GFC_ERR_GEOMETRY;
+    }
+    const size_t V = (size_t)ns * ns * ns * nt;
+    if (V * 4 >= (1ull << 31)) return GFC_ERR_GEOMETRY;
+    if (b->used_sites + V > b->max_sites) {
+        set_error("batch capacity: %zu sites in use, %zu requested, %zu maximum", b->used_sites, V, b->max_sites);
+        return GFC_ERR_BUSY;
+    }
+    int slot = -1;
+    for (int k = 0; k < b->max_slots; k++)
+        if (!b->used[k]) {
+            slot = k;
+            break;
+        }
+    if (slot < 0) {
+        set_error("batch has no free slot (%d in use)", b->max_slots);
+        return GFC_ERR_BUSY;
+    }
+    GFC_CHECK(cudaSetDevice(b->dev));
+    const size_t bytes = gfc_batch_slot_bytes(ns, nt);
+    void *m = nullptr;
+    cudaError_t e = cudaMallocAsync(&m, bytes, b->s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("device memory for a %d^3x%d slot (%zu bytes): %s", ns, nt, bytes, cudaGetErrorString(e));
+        return GFC_ERR_NOMEM;
+    }
+    BSlot sl{};
+    sl.l = make_lat(ns, nt);
+    const size_t vh = sl.l.vh;
+    char *p = (char *)m;
+    auto take = [&](size_t n) {
+        char *q = p;
+        p += al256(n);
+        return q;
+    };
+    sl.u = (double2 *)take(3 * 2 * vh * 9 * 16);
+    sl.ut = (double2 *)take(2 * vh * 9 * 16);
+    sl.g = (double2 *)take(2 * vh * 9 * 16);
+    sl.u64r = (double2 *)take(3 * 2 * vh * 6 * 16);
+    sl.g64r = (double2 *)take(2 * vh * 6 * 16);
+    sl.u32 = (float4 *)take(3 * 2 * vh * 3 * 16);
+    sl.g32 = (float4 *)take(2 * vh * 3 * 16);
+    sl.nbx = (int)(((sl.l.vs >> 1) + BCHUNK - 1) / BCHUNK);
+    sl.nfull = (int)((sl.l.vs + BCHUNK - 1) / BCHUNK);
+    sl.part = (double *)take((size_t)nt * sl.nbx * 2 * 8);
+    sl.tickets = (unsigned *)take((size_t)nt * 4);
+    GFC_CHECK(cudaMemsetAsync(sl.tickets, 0, (size_t)nt * 4, b->s));
+    GFC_CHECK(cudaMemcpyAsync(b->dslots + slot, &sl, sizeof sl, cudaMemcpyHostToDevice, b->s));
+    GFC_CHECK(cudaStreamSynchronize(b->s));   // the host copy of sl goes out of scope
+    b->hs[slot] = sl;
+    b->mem[slot] = m;
+    b->used[slot] = 1;
+    b->activated[slot] = 0;
+    b->ns[slot] = ns;
+    b->nt[slot] = nt;
+    b->used_sites += V;
+    // observables scratch large enough for every slot seen so far
+    size_t need = (size_t)nt * obs_blocks_per_slice(sl.l) * 4;
+    if (need > b->part_n) {
+        cudaFree(b->part);
+        b->part = nullptr;
+        GFC_CHECK(cudaMalloc(&b->part, need * sizeof(double)));
+        b->part_n = need;
+    }
+    *slot_out = slot;
+    return GFC_OK;
+}
+
+extern "C" int gfc_batch_remove(gfc_batch *b, int slot) {
+    if (!b || slot < 0 || slot >= b->max_slots || !b->used[slot]) return GFC_ERR_ARG;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    GFC_CHECK(cudaMemsetAsync(b->state + (size_t)slot * b->max_nt, 0, sizeof(int) * b->max_nt, b->s));
+    BSlot empty{};
+    GFC_CHECK(cudaMemcpyAsync(b->dslots + slot, &empty, sizeof empty, cudaMemcpyHostToDevice, b->s));
+    GFC_CHECK(cudaFreeAsync(b->mem[slot], b->s));
+    GFC_CHECK(cudaStreamSynchronize(b->s));
+    b->mem[slot] = nullptr;
+    b->used[slot] = 0;
+    b->used_sites -= (size_t)b->ns[slot] * b->ns[slot] * b->ns[slot] * b->nt[slot];
+    b->hs[slot] = BSlot{};
+    return GFC_OK;
+}
+
+static int check_slot(gfc_batch *b, int slot) {
+    if (!b || slot < 0 || slot >= b->max_slots || !b->used[slot]) return GFC_ERR_ARG;
+    return GFC_OK;
+}
+
+// Host links (reference layout, raw file bytes) into the slot, then reunitarised.
+extern "C" int gfc_batch_upload(gfc_batch *b, int slot, const void *host, int elem_bytes, int byteswap) {
+    int rc = check_slot(b, slot);
+    if (rc) return rc;
+    if (!host || (elem_bytes != 8 && elem_bytes != 4)) return GFC_ERR_ARG;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    const BSlot &sl = b->hs[slot];
+    const Lat &l = sl.l;
+    // stage through the slot's two-row FP64 field (not live before activation)
+    const size_t per_slice = (size_t)l.vs * 4 * 18 * elem_bytes;
+    // the working copies (u64r .. g32, contiguous) are dead outside a fix: >= 576 B per site
+    const size_t stage = (size_t)((char *)sl.part - (char *)sl.u64r);
+    const uint32_t per = (uint32_t)std::max<size_t>(1, stage / per_slice);
+    for (uint32_t t0 = 0; t0 < (uint32_t)l.nt; t0 += per) {
+        uint32_t n = std::min<uint32_t>(per, l.nt - t0);
+        GFC_CHECK(cudaMemcpyAsync(sl.u64r, (const char *)host + (size_t)t0 * per_slice, n * per_slice,
+                                  cudaMemcpyHostToDevice, b->s));
+        launch_load_links(sl.u64r, elem_bytes, byteswap, l, t0, n, sl.u, sl.ut, b->s);
+    }
+    launch_reunitarize(sl.u, l.vh, 3 * l.npar, b->status, b->s);
+    launch_reunitarize(sl.ut, l.vh, l.npar, b->status, b->s);
+    b->launches += 2 + (l.nt + per - 1) / per;
+    GFC_CHECK(cudaGetLastError());
+    return GFC_OK;
+}
+
+// The seeded synthetic configuration built on the device, then reunitarised.
+extern "C" int gfc_batch_synth(gfc_batch *b, int slot, uint64_t seed, double scale) {
+    int rc = check_slot(b, slot);
+    if (rc) return rc;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    const BSlot &sl = b->hs[slot];
+    launch_synth(sl.l, seed, scale, sl.g, sl.u, sl.ut, b->s);
+    launch_reunitarize(sl.u, sl.l.vh, 3 * sl.l.npar, b->status, b->s);
+    launch_reunitarize(sl.ut, sl.l.vh, sl.l.npar, b->status, b->s);
+    b->launches += 4;
+    GFC_CHECK(cudaGetLastError());
+    return GFC_OK;
+}
+
+// G = 1 and the working copies for the first round; precision GFC_PREC_MIXED
+// starts in FP32, anything else starts in FP64.
+extern "C" int gfc_batch_activate(gfc_batch *b, int slot, int precision) {
+    int rc = check_slot(b, slot);
+    if (rc) return rc;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    const BSlot &sl = b->hs[slot];
+    const Lat &l = sl.l;
+    launch_identity(sl.g, l, b->s);
+    int st;
+    if (precision == GFC_PREC_MIXED) {
+        launch_to_f32(sl.u, sl.u32, l.vh, 3 * l.npar, b->s);
+        launch_identity32(sl.g32, l.vh, l.npar, b->s);
+        st = SS_FP32;
+    } else {
+        launch_pack2(sl.u, sl.u64r, l.vh, 3 * l.npar, b->s);
+        launch_pack2(sl.g, sl.g64r, l.vh, l.npar, b->s);
+        st = SS_FP64;
+    }
+    BState bs{};
+    bs.nslices = b->nslices;
+    bs.state = b->state;
+    bs.sweeps = b->sweeps;
+    bs.ring = b->ring;
+    k_activate<<<(l.nt + 127) / 128, 128, 0, b->s>>>(bs, slot * b->max_nt, l.nt, st);
+    b->launches += 5;
+    b->activated[slot] = 1;
+    GFC_CHECK(cudaGetLastError());
+    return GFC_OK;
+}
+
+static BState make_state(gfc_batch *b, const gfc_params *p, const gfc_options *o) {
+    BState s;
+    memset(&s, 0, sizeof s);   // padding too: captured parameters are compared bytewise
+    s.slots = b->dslots;
+    s.max_nt = b->max_nt;
+    s.nslices = b->nslices;
+    s.state = b->state;
+    s.sweeps = b->sweeps;
+    s.ring = b->ring;
+    s.items32 = b->items32;
+    s.items64 = b->items64;
+    s.pend = b->pend;
+    s.cap_items = b->cap_items;
+    s.cap_pend = b->cap_pend;
+    s.counts = b->counts;
+    s.status = b->status;
+    s.omega = (double)p->omega_OR;
+    s.hits = p->hits;
+    const double tol = p->gfix_proxy == GFC_PROXY_THETA ? 6.0 * p->tolerance : p->tolerance;
+    s.tol = tol;
+    s.switch_e2 = std::max(o->switch_e2 > 0 ? o->switch_e2 : 1e-9, tol);
+    s.reunit64 = o->refine_reunit ? o->refine_reunit : p->sweeps_to_reunitarization;
+    s.reunit32 = std::min<unsigned>(p->sweeps_to_reunitarization, 50u);
+    return s;
+}
+
+template <class S>
+static void launch_bsweep(int minb, int grid, cudaStream_t st, const BState &bs) {
+    switch (minb) {
+        case 1: k_bsweep<S, 1><<<grid, BCHUNK, 0, st>>>(bs); break;
+        case 2: k_bsweep<S, 2><<<grid, BCHUNK, 0, st>>>(bs); break;
+        case 3: k_bsweep<S, 3><<<grid, BCHUNK, 0, st>>>(bs); break;
+        default: k_bsweep<S, 4><<<grid, BCHUNK, 0, st>>>(bs); break;
+    }
+}
+
+// enqueue one round on the stream (used for capture)
+static void enqueue_round(gfc_batch *b, const BState &bs) {
+    cudaStream_t st = b->s;
+    k_compact<<<1, 1024, 0, st>>>(bs);
+    k_switch_g<<<b->grid, BCHUNK, 0, st>>>(bs);
+    k_switch_u<<<b->grid, BCHUNK, 0, st>>>(bs);
+    k_switch_done<<<(b->nslices + 255) / 256, 256, 0, st>>>(bs);
+    for (int k = 0; k < b->round_k; k++) {
+        launch_bsweep<S32>(b->minb32, b->grid, st, bs);
+        launch_bsweep<S64R>(b->minb64, b->grid, st, bs);
+        k_btick<<<1, 32, 0, st>>>(bs);
+        k_breunit<S32><<<b->grid, BCHUNK, 0, st>>>(bs, bs.reunit32);
+        k_breunit<S64R><<<b->grid, BCHUNK, 0, st>>>(bs, bs.reunit64);
+    }
+}
+
+static int ensure_graph(gfc_batch *b, const gfc_params *p, const gfc_options *o) {
+    BState bs = make_state(b, p, o);
+    if (b->exec && !memcmp(&bs, &b->captured, sizeof bs)) return GFC_OK;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    GFC_CHECK(cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
+    enqueue_round(b, bs);
+    GFC_CHECK(cudaStreamEndCapture(b->s, &b->graph));
+    GFC_CHECK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    b->captured = bs;
+    return GFC_OK;
+}
+
+// One round (K half-sweeps of every active timeslice).  *active = timeslices still
+// working after it; the state table is copied back for gfc_batch_slot_status.
+extern "C" int gfc_batch_round(gfc_batch *b, const gfc_params *p, const gfc_options *o, int *active) {
+    if (!b || !p) return GFC_ERR_ARG;
+    gfc_options od;
+    if (!o) {
+        gfc_options_default(&od);
+        od.precision = GFC_PREC_MIXED;
+        o = &od;
+    }
+    GFC_CHECK(cudaSetDevice(b->dev));
+    int rc = ensure_graph(b, p, o);
+    if (rc) return rc;
+    GFC_CHECK(cudaGraphLaunch(b->exec, b->s));
+    b->launches += 4 + 5 * b->round_k;
+    b->rounds++;
+    GFC_CHECK(cudaMemcpyAsync(b->hcounts, b->counts, sizeof(int) * 8, cudaMemcpyDeviceToHost, b->s));
+    GFC_CHECK(cudaMemcpyAsync(b->hstate, b->state, sizeof(int) * b->nslices, cudaMemcpyDeviceToHost, b->s));
+    GFC_CHECK(cudaStreamSynchronize(b->s));
+    if (b->hcounts[5]) {
+        set_error("batch work list overflow");
+        return GFC_ERR_STATE;
+    }
+    // active timeslices after the round (the count in hcounts[3] is from its start)
+    int act = 0;
+    for (int g = 0; g < b->nslices; g++) act += b->hstate[g] != SS_EMPTY && b->hstate[g] != SS_DONE;
+    if (active) *active = act;
+    return GFC_OK;
+}
+
+// 1 if every timeslice of the slot has retired (from the state copied by the last round)
+extern "C" int gfc_batch_slot_done(gfc_batch *b, int slot, int *done) {
+    int rc = check_slot(b, slot);
+    if (rc) return rc;
+    if (!done) return GFC_ERR_ARG;
+    int d = b->activated[slot];
+    for (int t = 0; t < b->nt[slot] && d; t++) d = b->hstate[(size_t)slot * b->max_nt + t] == SS_DONE;
+    *done = d;
+    return GFC_OK;
+}
+
+// After retirement: canonical FP64 links and G, reunitarised; temporal links
+// transformed; report with the largest per-timeslice half-sweep count and the
+// observables of the fixed lattice.
+extern "C" int gfc_batch_finalize(gfc_batch *b, int slot, gfc_report *r) {
+    int rc = check_slot(b, slot);
+    if (rc) return rc;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    const BSlot &sl = b->hs[slot];
+    const Lat &l = sl.l;
+    k_set_state<<<(l.nt + 127) / 128, 128, 0, b->s>>>(b->state, slot * b->max_nt, l.nt, SS_DONE);
+    launch_unpack2(sl.u64r, sl.u, l.vh, 3 * l.npar, b->s);
+    launch_unpack2(sl.g64r, sl.g, l.vh, l.npar, b->s);
+    launch_reunitarize(sl.u, l.vh, 3 * l.npar, b->status, b->s);
+    launch_reunitarize(sl.g, l.vh, l.npar, b->status, b->s);
+    launch_temporal_transform(sl.ut, sl.g, l, b->s);
+    launch_reunitarize(sl.ut, l.vh, l.npar, b->status, b->s);
+    b->launches += 6;
+    if (r) {
+        memset(r, 0, sizeof *r);
+        std::vector<int> sw(l.nt);
+        GFC_CHECK(cudaMemcpyAsync(sw.data(), b->sweeps + (size_t)slot * b->max_nt, sizeof(int) * l.nt,
+                                  cudaMemcpyDeviceToHost, b->s));
+        launch_obs(sl.u, l, b->part, b->dres, nullptr, b->s);
+        launch_functional(sl.u, l, b->part, b->dres + 2, b->s);
+        b->launches += 4;
+        GFC_CHECK(cudaMemcpyAsync(b->hres, b->dres, sizeof(double) * 3, cudaMemcpyDeviceToHost, b->s));
+        GFC_CHECK(cudaStreamSynchronize(b->s));
+        int mx = 0;
+        long long tot = 0;
+        for (int t = 0; t < l.nt; t++) {
+            mx = std::max(mx, sw[t]);
+            tot += sw[t];
+        }
+        r->sweeps = mx;
+        r->site_updates = tot * (long long)(l.vs / 2);
+        r->e2 = b->hres[0] / (double)l.v;
+        r->theta = b->hres[1] / (3.0 * (double)l.v);
+        r->functional = b->hres[2] / ((double)l.v * 9.0);
+        r->final_residue = r->e2;
+        r->status = mx;
+    }
+    GFC_CHECK(cudaGetLastError());
+    b->activated[slot] = 0;
+    return GFC_OK;
+}
+
+extern "C" int gfc_batch_plaquette(gfc_batch *b, int slot, double *spatial, double *temporal) {
+    int rc = check_slot(b, slot);
+    if (rc) return rc;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    const BSlot &sl = b->hs[slot];
+    launch_plaquette(sl.u, sl.ut, sl.l, b->part, b->dres, b->s);
+    GFC_CHECK(cudaMemcpyAsync(b->hres, b->dres, sizeof(double) * 2, cudaMemcpyDeviceToHost, b->s));
+    GFC_CHECK(cudaStreamSynchronize(b->s));
+    if (spatial) *spatial = b->hres[0] / (3.0 * (double)sl.l.v);
+    if (temporal) *temporal = b->hres[1] / (3.0 * (double)sl.l.v);
+    return GFC_OK;
+}
+
+extern "C" int gfc_batch_download_gt(gfc_batch *b, int slot, void *host, int elem_bytes, int byteswap) {
+    int rc = check_slot(b, slot);
+    if (rc) return rc;
+    if (b->activated[slot]) {
+        set_error("slot %d is still being fixed (finalize it first)", slot);
+        return GFC_ERR_STATE;
+    }
+    if (!host || (elem_bytes != 8 && elem_bytes != 4)) return GFC_ERR_ARG;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    const BSlot &sl = b->hs[slot];
+    const Lat &l = sl.l;
+    // raw output staged through the (dead) FP64 two-row field
+    const size_t per_slice = (size_t)l.vs * 18 * elem_bytes;
+    // the working copies (u64r .. g32, contiguous) are dead outside a fix: >= 576 B per site
+    const size_t stage = (size_t)((char *)sl.part - (char *)sl.u64r);
+    const uint32_t per = (uint32_t)std::max<size_t>(1, stage / per_slice);
+    for (uint32_t t0 = 0; t0 < (uint32_t)l.nt; t0 += per) {
+        uint32_t n = std::min<uint32_t>(per, l.nt - t0);
+        launch_store_gt(sl.g, l, t0, n, elem_bytes, byteswap, sl.u64r, b->s);
+        GFC_CHECK(cudaMemcpyAsync((char *)host + (size_t)t0 * per_slice, sl.u64r, n * per_slice,
+                                  cudaMemcpyDeviceToHost, b->s));
+    }
+    GFC_CHECK(cudaStreamSynchronize(b->s));
+    return GFC_OK;
+}
+
+extern "C" int gfc_batch_download_links(gfc_batch *b, int slot, void *host, int elem_bytes, int byteswap) {
+    int rc = check_slot(b, slot);
+    if (rc) return rc;
+    if (b->activated[slot]) {
+        set_error("slot %d is still being fixed (finalize it first)", slot);
+        return GFC_ERR_STATE;
+    }
+    if (!host || (elem_bytes != 8 && elem_bytes != 4)) return GFC_ERR_ARG;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    const BSlot &sl = b->hs[slot];
+    const Lat &l = sl.l;
+    const size_t per_slice = (size_t)l.vs * 4 * 18 * elem_bytes;
+    // the working copies (u64r .. g32, contiguous) are dead outside a fix: >= 576 B per site
+    const size_t stage = (size_t)((char *)sl.part - (char *)sl.u64r);
+    const uint32_t per = (uint32_t)std::max<size_t>(1, stage / per_slice);
+    for (uint32_t t0 = 0; t0 < (uint32_t)l.nt; t0 += per) {
+        uint32_t n = std::min<uint32_t>(per, l.nt - t0);
+        launch_store_links(sl.u, sl.ut, l, t0, n, elem_bytes, byteswap, sl.u64r, b->s);
+        GFC_CHECK(cudaMemcpyAsync((char *)host + (size_t)t0 * per_slice, sl.u64r, n * per_slice,
+                                  cudaMemcpyDeviceToHost, b->s));
+    }
+    GFC_CHECK(cudaStreamSynchronize(b->s));
+    return GFC_OK;
+}
+
+// half-sweeps each timeslice of the slot has received (nt values)
+extern "C" int gfc_batch_slice_sweeps(gfc_batch *b, int slot, int *out) {
+    int rc = check_slot(b, slot);
+    if (rc) return rc;
+    if (!out) return GFC_ERR_ARG;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    GFC_CHECK(cudaMemcpyAsync(out, b->sweeps + (size_t)slot * b->max_nt, sizeof(int) * b->nt[slot],
+                              cudaMemcpyDeviceToHost, b->s));
+    GFC_CHECK(cudaStreamSynchronize(b->s));
+    return GFC_OK;
+}
+
+extern "C" int gfc_batch_status(gfc_batch *b, unsigned *status) {
+    if (!b || !status) return GFC_ERR_ARG;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    GFC_CHECK(cudaMemcpy(status, b->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    GFC_CHECK(cudaMemset(b->status, 0, sizeof(unsigned)));
+    return GFC_OK;
+}
+
+extern "C" long long gfc_batch_kernel_launches(const gfc_batch *b) { return b ? b->launches : -1; }
+extern "C" void *gfc_batch_stream(gfc_batch *b) { return b ? (void *)b->s : nullptr; }
+
+// launch shape (minimum resident CTAs per SM) of the two sweep kernels and the
+// half-sweeps per captured round
+extern "C" int gfc_batch_set_shape(gfc_batch *b, int minb32, int minb64, int round_sweeps) {
+    if (!b || minb32 < 1 || minb32 > 4 || minb64 < 1 || minb64 > 4 || round_sweeps < 1 || round_sweeps > 64)
+        return GFC_ERR_ARG;
+    b->minb32 = minb32;
+    b->minb64 = minb64;
+    b->round_k = round_sweeps;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return GFC_OK;
+}
+
+// Run every activated slot to retirement (or max_sweeps) and finalise it.
+// reports[slot] is filled for every slot that was active; returns the number of
+// rounds, or an error.
+extern "C" int gfc_batch_fix_all(gfc_batch *b, const gfc_params *p, const gfc_options *o, gfc_report *reports) {
+    if (!b || !p) return GFC_ERR_ARG;
+    if (!gfc_params_valid(p)) return GFC_FIX_BAD_PARAMS;
+    std::vector<int> act(b->max_slots, 0);
+    for (int s = 0; s < b->max_slots; s++) act[s] = b->used[s] && b->activated[s];
+    const int max_rounds = (int)(p->max_sweeps_to_fix / (unsigned)b->round_k) + 1;
+    int rounds = 0, active = 1;
+    while (active > 0 && rounds < max_rounds) {
+        int rc = gfc_batch_round(b, p, o, &active);
+        if (rc) return rc;
+        rounds++;
+    }
+    for (int s = 0; s < b->max_slots; s++)
+        if (act[s]) {
+            int done = 0;
+            gfc_batch_slot_done(b, s, &done);
+            int rc = gfc_batch_finalize(b, s, reports ? reports + s : nullptr);
+            if (rc) return rc;
+            if (reports && !done) reports[s].status = GFC_FIX_NOT_CONVERGED;
+        }
+    return rounds;
+}

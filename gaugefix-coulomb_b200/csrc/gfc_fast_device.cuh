@@ -1,0 +1,414 @@
+// gfc_fast_device.cuh -- device building blocks of the fast sweep kernels
+// (storage policies, the direct-accumulation update, row-wise application with
+// the fused e2 components).  Shared by the single-lattice kernels (gfc_fast.cu)
+// and the batch engine (gfc_batch.cu).
+#pragma once
+#include "gfc_device.cuh"
+
+namespace gfc {
+
+template <typename T>
+struct CT;
+template <>
+struct CT<double> {
+    using t = double2;
+};
+template <>
+struct CT<float> {
+    using t = float2;
+};
+
+template <typename T>
+struct Mt {
+    typename CT<T>::t e[9];
+};
+
+template <typename C>
+__device__ __forceinline__ C mkc(decltype(C::x) a, decltype(C::x) b) {
+    C r;
+    r.x = a;
+    r.y = b;
+    return r;
+}
+template <typename C>
+__device__ __forceinline__ C fmul(C a, C b) {
+    return mkc<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C>
+__device__ __forceinline__ C fmul_conj(C a, C b) {  // a * conj(b)
+    return mkc<C>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+template <typename C>
+__device__ __forceinline__ C fadd(C a, C b) {
+    return mkc<C>(a.x + b.x, a.y + b.y);
+}
+template <typename C>
+__device__ __forceinline__ C fconj(C a) {
+    return mkc<C>(a.x, -a.y);
+}
+
+__device__ __forceinline__ double frsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float frsqrt(float x) { return rsqrtf(x); }
+
+// conj(a x b)
+template <typename C>
+__device__ __forceinline__ void fcross_conj(const C *a, const C *b, C *o) {
+    o[0] = fconj(fadd(fmul(a[1], b[2]), mkc<C>(-(a[2].x * b[1].x - a[2].y * b[1].y), -(a[2].x * b[1].y + a[2].y * b[1].x))));
+    o[1] = fconj(fadd(fmul(a[2], b[0]), mkc<C>(-(a[0].x * b[2].x - a[0].y * b[2].y), -(a[0].x * b[2].y + a[0].y * b[2].x))));
+    o[2] = fconj(fadd(fmul(a[0], b[1]), mkc<C>(-(a[1].x * b[0].x - a[1].y * b[0].y), -(a[1].x * b[0].y + a[1].y * b[0].x))));
+}
+
+template <typename T>
+__device__ __forceinline__ void reconstruct_row2(Mt<T> &m) {
+    fcross_conj(&m.e[0], &m.e[3], &m.e[6]);
+}
+
+// ---------------------------------------------------------------- storage --
+struct S64 {
+    using T = double;
+    using V = double2;
+    static constexpr int NS = 9;
+    static constexpr int BYTES = 144;
+    __device__ static void load(const V *__restrict__ p, size_t st, Mt<T> &m) {
+#pragma unroll
+        for (int c = 0; c < 9; c++) m.e[c] = p[(size_t)c * st];
+    }
+    __device__ static void load_rows01(const V *__restrict__ p, size_t st, Mt<T> &m) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) m.e[c] = p[(size_t)c * st];
+    }
+    __device__ static void store(V *__restrict__ p, size_t st, const Mt<T> &m) {
+#pragma unroll
+        for (int c = 0; c < 9; c++) p[(size_t)c * st] = m.e[c];
+    }
+    static constexpr bool ROWS01_ONLY = false;
+    static constexpr bool ROWWISE = true;
+    static constexpr int STORED_ROWS = 3;
+};
+
+// FP64, rows 0 and 1 only (6 double2 per matrix, 96 B); row 2 rebuilt as conj(r0 x r1)
+struct S64R {
+    using T = double;
+    using V = double2;
+    static constexpr int NS = 6;
+    static constexpr int BYTES = 96;
+    __device__ static void load_rows01(const V *__restrict__ p, size_t st, Mt<T> &m) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) m.e[c] = p[(size_t)c * st];
+    }
+    __device__ static void load(const V *__restrict__ p, size_t st, Mt<T> &m) {
+        load_rows01(p, st, m);
+        reconstruct_row2(m);
+    }
+    __device__ static void store(V *__restrict__ p, size_t st, const Mt<T> &m) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) p[(size_t)c * st] = m.e[c];
+    }
+    static constexpr bool ROWS01_ONLY = true;
+    static constexpr bool ROWWISE = true;
+    static constexpr int STORED_ROWS = 2;
+};
+
+struct S32 {
+    using T = float;
+    using V = float4;
+    static constexpr int NS = 3;
+    static constexpr int BYTES = 48;
+    __device__ static void load_rows01(const V *__restrict__ p, size_t st, Mt<T> &m) {
+        float4 a = p[0], b = p[st], c = p[2 * st];
+        m.e[0] = make_float2(a.x, a.y);
+        m.e[1] = make_float2(a.z, a.w);
+        m.e[2] = make_float2(b.x, b.y);
+        m.e[3] = make_float2(b.z, b.w);
+        m.e[4] = make_float2(c.x, c.y);
+        m.e[5] = make_float2(c.z, c.w);
+    }
+    __device__ static void load(const V *__restrict__ p, size_t st, Mt<T> &m) {
+        load_rows01(p, st, m);
+        reconstruct_row2(m);
+    }
+    __device__ static void store(V *__restrict__ p, size_t st, const Mt<T> &m) {
+        p[0] = make_float4(m.e[0].x, m.e[0].y, m.e[1].x, m.e[1].y);
+        p[st] = make_float4(m.e[2].x, m.e[2].y, m.e[3].x, m.e[3].y);
+        p[2 * st] = make_float4(m.e[4].x, m.e[4].y, m.e[5].x, m.e[5].y);
+    }
+    static constexpr bool ROWS01_ONLY = true;
+    static constexpr bool ROWWISE = false;
+    static constexpr int STORED_ROWS = 2;
+};
+
+template <class S>
+__device__ __forceinline__ size_t su_idx(const Lat &l, int d, int par, uint32_t i) {
+    return ((size_t)(d * l.npar + par) * S::NS) * l.vh + i;
+}
+template <class S>
+__device__ __forceinline__ size_t sg_idx(const Lat &l, int par, uint32_t i) {
+    return ((size_t)par * S::NS) * l.vh + i;
+}
+
+// ------------------------------------------------------------- the update --
+// e2 density of a site from its w (see the header comment)
+template <typename T>
+__device__ __forceinline__ double e2_from_w(const Mt<T> &w) {
+    double c1 = (double)w.e[1].y + (double)w.e[3].y;
+    double c2 = (double)w.e[1].x - (double)w.e[3].x;
+    double c3 = (double)w.e[0].y - (double)w.e[4].y;
+    double c4 = (double)w.e[2].y + (double)w.e[6].y;
+    double c5 = (double)w.e[2].x - (double)w.e[6].x;
+    double c6 = (double)w.e[5].y + (double)w.e[7].y;
+    double c7 = (double)w.e[5].x - (double)w.e[7].x;
+    double c8 = ((double)w.e[0].y + (double)w.e[4].y - 2.0 * (double)w.e[8].y) * 0.57735026918962576451;
+    return c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4 + c5 * c5 + c6 * c6 + c7 * c7 + c8 * c8;
+}
+
+// one Cabibbo-Marinari hit on rows (A, B) of w, accumulated into g
+template <int A, int B, typename T>
+__device__ __forceinline__ void fsub_hit(Mt<T> &w, Mt<T> &g) {
+    using C = typename CT<T>::t;
+    T k0 = w.e[EL(A, A)].x + w.e[EL(B, B)].x;
+    T k1 = -(w.e[EL(A, B)].y + w.e[EL(B, A)].y);
+    T k2 = -(w.e[EL(A, B)].x - w.e[EL(B, A)].x);
+    T k3 = -(w.e[EL(A, A)].y - w.e[EL(B, B)].y);
+    T n = k0 * k0 + k1 * k1 + k2 * k2 + k3 * k3;
+    if (n == T(0)) return;
+    T r = frsqrt(n);
+    k0 *= r;
+    k1 *= r;
+    k2 *= r;
+    k3 *= r;
+    const C x00 = mkc<C>(k0, k3), x01 = mkc<C>(k2, k1), x10 = mkc<C>(-k2, k1), x11 = mkc<C>(k0, -k3);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        C a = w.e[EL(A, c)], b = w.e[EL(B, c)];
+        w.e[EL(A, c)] = fadd(fmul(x00, a), fmul(x01, b));
+        w.e[EL(B, c)] = fadd(fmul(x10, a), fmul(x11, b));
+        a = g.e[EL(A, c)];
+        b = g.e[EL(B, c)];
+        g.e[EL(A, c)] = fadd(fmul(x00, a), fmul(x01, b));
+        g.e[EL(B, c)] = fadd(fmul(x10, a), fmul(x11, b));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ bool fproject(Mt<T> &m) {
+    using C = typename CT<T>::t;
+    T n0 = m.e[0].x * m.e[0].x + m.e[0].y * m.e[0].y + m.e[1].x * m.e[1].x + m.e[1].y * m.e[1].y +
+           m.e[2].x * m.e[2].x + m.e[2].y * m.e[2].y;
+    if (n0 == T(0)) return false;
+    T r0 = frsqrt(n0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) m.e[k] = mkc<C>(m.e[k].x * r0, m.e[k].y * r0);
+    fcross_conj(&m.e[0], &m.e[3], &m.e[6]);
+    T n2 = m.e[6].x * m.e[6].x + m.e[6].y * m.e[6].y + m.e[7].x * m.e[7].x + m.e[7].y * m.e[7].y +
+           m.e[8].x * m.e[8].x + m.e[8].y * m.e[8].y;
+    if (n2 == T(0)) return false;
+    T r2 = frsqrt(n2);
+#pragma unroll
+    for (int k = 6; k < 9; k++) m.e[k] = mkc<C>(m.e[k].x * r2, m.e[k].y * r2);
+    fcross_conj(&m.e[6], &m.e[0], &m.e[3]);
+    return true;
+}
+
+template <typename T>
+__device__ __forceinline__ void fidentity(Mt<T> &m) {
+    using C = typename CT<T>::t;
+#pragma unroll
+    for (int k = 0; k < 9; k++) m.e[k] = mkc<C>((k % 4) == 0 ? T(1) : T(0), T(0));
+}
+
+// upd = Proj_SU3(I + omega (g - I)), g = w_final w^-1 accumulated by the hits
+template <typename T>
+__device__ __forceinline__ void fupdate(Mt<T> &w, T omega, unsigned hits, Mt<T> &g) {
+    using C = typename CT<T>::t;
+    fidentity(g);
+#pragma unroll 1
+    for (unsigned h = 0; h < hits; h++) {
+        fsub_hit<0, 1>(w, g);
+        fsub_hit<0, 2>(w, g);
+        fsub_hit<1, 2>(w, g);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            C x = g.e[EL(a, b)];
+            g.e[EL(a, b)] = a == b ? mkc<C>(T(1) + omega * (x.x - T(1)), omega * x.y) : mkc<C>(omega * x.x, omega * x.y);
+        }
+    if (!fproject(g)) fidentity(g);
+}
+
+// c = a . b for the rows of c that storage S keeps
+template <class S, typename T>
+__device__ __forceinline__ void fprod_left(const Mt<T> &a, const Mt<T> &b, Mt<T> &c) {
+    using C = typename CT<T>::t;
+    constexpr int NR = S::ROWS01_ONLY ? 2 : 3;
+#pragma unroll
+    for (int i = 0; i < NR; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            C s = fmul(a.e[EL(i, 0)], b.e[EL(0, j)]);
+            s = fadd(s, fmul(a.e[EL(i, 1)], b.e[EL(1, j)]));
+            s = fadd(s, fmul(a.e[EL(i, 2)], b.e[EL(2, j)]));
+            c.e[EL(i, j)] = s;
+        }
+}
+// c = a . b^dagger (row-local in a: only the stored rows of a are needed)
+template <class S, typename T>
+__device__ __forceinline__ void fprod_dag(const Mt<T> &a, const Mt<T> &b, Mt<T> &c) {
+    using C = typename CT<T>::t;
+    constexpr int NR = S::ROWS01_ONLY ? 2 : 3;
+#pragma unroll
+    for (int i = 0; i < NR; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            C s = fmul_conj(a.e[EL(i, 0)], b.e[EL(j, 0)]);
+            s = fadd(s, fmul_conj(a.e[EL(i, 1)], b.e[EL(j, 1)]));
+            s = fadd(s, fmul_conj(a.e[EL(i, 2)], b.e[EL(j, 2)]));
+            c.e[EL(i, j)] = s;
+        }
+}
+
+// Contribution of row i = (o0, o1, o2) of a matrix o added to w (sign +1) or of
+// o^dagger added to w (sign -1) to the 8 algebra components of w's e2 density:
+//   c1 = Im w01 + Im w10, c2 = Re w01 - Re w10, c3 = Im w00 - Im w11,
+//   c4 = Im w02 + Im w20, c5 = Re w02 - Re w20, c6 = Im w12 + Im w21,
+//   c7 = Re w12 - Re w21, c8 = Im w00 + Im w11 - 2 Im w22 (times 1/sqrt 3 later).
+// Adding o^dagger contributes exactly the negative of adding o.
+template <int I, typename C>
+__device__ __forceinline__ void acc_row(double (&c)[8], C o0, C o1, C o2, double s) {
+    if (I == 0) {
+        c[0] += s * o1.y;
+        c[1] += s * o1.x;
+        c[2] += s * o0.y;
+        c[3] += s * o2.y;
+        c[4] += s * o2.x;
+        c[7] += s * o0.y;
+    } else if (I == 1) {
+        c[0] += s * o0.y;
+        c[1] -= s * o0.x;
+        c[2] -= s * o1.y;
+        c[5] += s * o2.y;
+        c[6] += s * o2.x;
+        c[7] += s * o1.y;
+    } else {
+        c[3] += s * o0.y;
+        c[4] -= s * o0.x;
+        c[5] += s * o1.y;
+        c[6] -= s * o1.x;
+        c[7] -= 2.0 * s * o2.y;
+    }
+}
+
+template <int I, typename T>
+__device__ __forceinline__ void acc_mat_row(double (&c)[8], const Mt<T> &o, double s) {
+    acc_row<I>(c, o.e[EL(I, 0)], o.e[EL(I, 1)], o.e[EL(I, 2)], s);
+}
+
+// f <- up . f for a forward link; FP64 works one row at a time to keep few values live
+template <class S>
+__device__ __forceinline__ void apply_forward(typename S::V *__restrict__ p, size_t st,
+                                              const Mt<typename S::T> &up, int track, double (&cc)[8]) {
+    using T = typename S::T;
+    using C = typename CT<T>::t;
+    Mt<T> f;
+    S::load(p, st, f);
+    if constexpr (S::ROWWISE) {
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (r >= S::STORED_ROWS && !track) break;   // row 2 of a two-row link: e2 only
+            C o[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C s = fmul(up.e[EL(r, 0)], f.e[EL(0, j)]);
+                s = fadd(s, fmul(up.e[EL(r, 1)], f.e[EL(1, j)]));
+                s = fadd(s, fmul(up.e[EL(r, 2)], f.e[EL(2, j)]));
+                o[j] = s;
+                if (r < S::STORED_ROWS) p[(size_t)(3 * r + j) * st] = s;
+            }
+            if (track) {
+                if (r == 0) acc_row<0>(cc, o[0], o[1], o[2], 1.0);
+                if (r == 1) acc_row<1>(cc, o[0], o[1], o[2], 1.0);
+                if (r == 2) acc_row<2>(cc, o[0], o[1], o[2], 1.0);
+            }
+        }
+    } else {
+        Mt<T> o;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C s = fmul(up.e[EL(r, 0)], f.e[EL(0, j)]);
+                s = fadd(s, fmul(up.e[EL(r, 1)], f.e[EL(1, j)]));
+                s = fadd(s, fmul(up.e[EL(r, 2)], f.e[EL(2, j)]));
+                o.e[EL(r, j)] = s;
+            }
+        S::store(p, st, o);
+        if (track) {
+            acc_mat_row<0>(cc, o, 1.0);
+            acc_mat_row<1>(cc, o, 1.0);
+            acc_mat_row<2>(cc, o, 1.0);
+        }
+    }
+}
+
+// r <- r . up^dagger for a backward link (row-local)
+template <class S>
+__device__ __forceinline__ void apply_backward(typename S::V *__restrict__ p, size_t st,
+                                               const Mt<typename S::T> &up, int track, double (&cc)[8]) {
+    using T = typename S::T;
+    using C = typename CT<T>::t;
+    if constexpr (S::ROWWISE) {
+        C rows[3][3];   // rows of the old link; row 2 of a two-row link is rebuilt for e2
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (r >= S::STORED_ROWS) {
+                if (!track) break;
+                fcross_conj(rows[0], rows[1], rows[2]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 3; j++) rows[r][j] = p[(size_t)(3 * r + j) * st];
+            }
+            const C a0 = rows[r][0], a1 = rows[r][1], a2 = rows[r][2];
+            C o[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C s = fmul_conj(a0, up.e[EL(j, 0)]);
+                s = fadd(s, fmul_conj(a1, up.e[EL(j, 1)]));
+                s = fadd(s, fmul_conj(a2, up.e[EL(j, 2)]));
+                o[j] = s;
+                if (r < S::STORED_ROWS) p[(size_t)(3 * r + j) * st] = s;
+            }
+            if (track) {
+                if (r == 0) acc_row<0>(cc, o[0], o[1], o[2], -1.0);
+                if (r == 1) acc_row<1>(cc, o[0], o[1], o[2], -1.0);
+                if (r == 2) acc_row<2>(cc, o[0], o[1], o[2], -1.0);
+            }
+        }
+    } else {
+        Mt<T> m, o;
+        if (track)
+            S::load(p, st, m);
+        else
+            S::load_rows01(p, st, m);
+        const int nr = track ? 3 : 2;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (r >= nr) break;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C s = fmul_conj(m.e[EL(r, 0)], up.e[EL(j, 0)]);
+                s = fadd(s, fmul_conj(m.e[EL(r, 1)], up.e[EL(j, 1)]));
+                s = fadd(s, fmul_conj(m.e[EL(r, 2)], up.e[EL(j, 2)]));
+                o.e[EL(r, j)] = s;
+            }
+        }
+        S::store(p, st, o);
+        if (track) {
+            acc_mat_row<0>(cc, o, -1.0);
+            acc_mat_row<1>(cc, o, -1.0);
+            acc_mat_row<2>(cc, o, -1.0);
+        }
+    }
+}
+
+}  // namespace gfc

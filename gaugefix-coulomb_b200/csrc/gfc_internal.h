@@ -40,6 +40,15 @@ void launch_store_links(const double2 *u, const double2 *ut, const Lat &l, uint3
 void launch_temporal_transform(double2 *ut, const double2 *g, const Lat &l, cudaStream_t s);
 // u_d(x) <- G(x) u0_d(x) G(x+d)^dagger for the spatial links (rebuild from originals)
 void launch_apply_gt_spatial(double2 *u, const double2 *u0, const double2 *g, const Lat &l, cudaStream_t s);
+// format conversions over nblk SoA blocks of `stride` matrices (gfc_fast.cu)
+void launch_to_f32(const double2 *src, float4 *dst, uint32_t stride, uint32_t nblk, cudaStream_t s);
+void launch_identity32(float4 *g, uint32_t stride, uint32_t nblk, cudaStream_t s);
+void launch_pack2(const double2 *src, double2 *dst, uint32_t stride, uint32_t nblk, cudaStream_t s);
+void launch_unpack2(const double2 *src, double2 *dst, uint32_t stride, uint32_t nblk, cudaStream_t s);
+// seeded synthetic links built on the device (gfc_synth_dev.cu); gtmp is a
+// G-sized scratch field (overwritten)
+void launch_synth(const Lat &l, uint64_t seed, double scale, double2 *gtmp, double2 *u, double2 *ut,
+                  cudaStream_t s);
 // plaquette partials: [nt][nbx][2] = (spatial sum, temporal sum) of Re Tr/3
 void launch_plaquette(const double2 *u, const double2 *ut, const Lat &l, double *part, double *out,
                       cudaStream_t s);

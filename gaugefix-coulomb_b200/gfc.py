@@ -361,3 +361,152 @@ def gaugefix_overrelaxation(U, G, ns, nt, params=None, opts=None, device=0):
             lat.download_links(8, False, out=U)
             lat.download_gt(8, False, out=G)
     return rc, rep
+
+
+# ---------------------------------------------------------------- batches --
+def _bind_batch():
+    P, I, D, S = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+    IP = ctypes.POINTER(ctypes.c_int)
+    RP = ctypes.POINTER(Report)
+    sig = {
+        "gfc_batch_create": (I, [I, S, I, I, ctypes.POINTER(P)]),
+        "gfc_batch_destroy": (I, [P]),
+        "gfc_batch_slot_bytes": (S, [I, I]),
+        "gfc_batch_add": (I, [P, I, I, IP]),
+        "gfc_batch_remove": (I, [P, I]),
+        "gfc_batch_upload": (I, [P, I, P, I, I]),
+        "gfc_batch_synth": (I, [P, I, ctypes.c_uint64, D]),
+        "gfc_batch_activate": (I, [P, I, I]),
+        "gfc_batch_round": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), IP]),
+        "gfc_batch_slot_done": (I, [P, I, IP]),
+        "gfc_batch_finalize": (I, [P, I, RP]),
+        "gfc_batch_plaquette": (I, [P, I, ctypes.POINTER(D), ctypes.POINTER(D)]),
+        "gfc_batch_download_gt": (I, [P, I, P, I, I]),
+        "gfc_batch_download_links": (I, [P, I, P, I, I]),
+        "gfc_batch_status": (I, [P, ctypes.POINTER(ctypes.c_uint)]),
+        "gfc_batch_slice_sweeps": (I, [P, I, P]),
+        "gfc_batch_kernel_launches": (ctypes.c_longlong, [P]),
+        "gfc_batch_stream": (P, [P]),
+        "gfc_batch_set_shape": (I, [P, I, I, I]),
+        "gfc_batch_fix_all": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), RP]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+
+
+_bind_batch()
+
+
+class Batch:
+    """Many lattices on one GPU, swept timeslice by timeslice (a gfc_batch)."""
+
+    def __init__(self, max_sites, max_slots=128, max_nt=128, device=0):
+        h = ctypes.c_void_p()
+        _check(lib.gfc_batch_create(device, int(max_sites), max_slots, max_nt, ctypes.byref(h)), "gfc_batch_create")
+        self.h = h
+        self.max_slots = max_slots
+        self.geom = {}
+
+    def close(self):
+        if self.h:
+            lib.gfc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @staticmethod
+    def slot_bytes(ns, nt):
+        return lib.gfc_batch_slot_bytes(ns, nt)
+
+    def add(self, ns, nt):
+        s = ctypes.c_int()
+        _check(lib.gfc_batch_add(self.h, ns, nt, ctypes.byref(s)), "gfc_batch_add")
+        self.geom[s.value] = (ns, nt)
+        return s.value
+
+    def remove(self, slot):
+        _check(lib.gfc_batch_remove(self.h, slot), "gfc_batch_remove")
+        self.geom.pop(slot, None)
+
+    def upload(self, slot, buf, elem_bytes=8, byteswap=False):
+        a = np.ascontiguousarray(buf)
+        ns, nt = self.geom[slot]
+        assert a.nbytes == ns ** 3 * nt * 4 * 18 * elem_bytes
+        _check(lib.gfc_batch_upload(self.h, slot, a.ctypes.data, elem_bytes, int(byteswap)), "gfc_batch_upload")
+
+    def synth(self, slot, seed, scale):
+        _check(lib.gfc_batch_synth(self.h, slot, seed, scale), "gfc_batch_synth")
+
+    def activate(self, slot, precision=PREC_MIXED):
+        _check(lib.gfc_batch_activate(self.h, slot, precision), "gfc_batch_activate")
+
+    def round(self, params, opts):
+        a = ctypes.c_int()
+        _check(lib.gfc_batch_round(self.h, ctypes.byref(params), ctypes.byref(opts), ctypes.byref(a)), "round")
+        return a.value
+
+    def slot_done(self, slot):
+        d = ctypes.c_int()
+        _check(lib.gfc_batch_slot_done(self.h, slot, ctypes.byref(d)), "slot_done")
+        return bool(d.value)
+
+    def finalize(self, slot):
+        r = Report()
+        _check(lib.gfc_batch_finalize(self.h, slot, ctypes.byref(r)), "finalize")
+        return r
+
+    def plaquette(self, slot):
+        s, t = ctypes.c_double(), ctypes.c_double()
+        _check(lib.gfc_batch_plaquette(self.h, slot, ctypes.byref(s), ctypes.byref(t)), "plaquette")
+        return s.value, t.value
+
+    def download_gt(self, slot, elem_bytes=8, byteswap=False):
+        ns, nt = self.geom[slot]
+        out = np.empty(ns ** 3 * nt * 18, dtype=np.float64 if elem_bytes == 8 else np.float32)
+        _check(lib.gfc_batch_download_gt(self.h, slot, out.ctypes.data, elem_bytes, int(byteswap)), "download_gt")
+        return out
+
+    def download_links(self, slot, elem_bytes=8, byteswap=False):
+        ns, nt = self.geom[slot]
+        out = np.empty(ns ** 3 * nt * 4 * 18, dtype=np.float64 if elem_bytes == 8 else np.float32)
+        _check(lib.gfc_batch_download_links(self.h, slot, out.ctypes.data, elem_bytes, int(byteswap)),
+               "download_links")
+        return out
+
+    def slice_sweeps(self, slot):
+        ns, nt = self.geom[slot]
+        out = np.empty(nt, dtype=np.int32)
+        _check(lib.gfc_batch_slice_sweeps(self.h, slot, out.ctypes.data), "slice_sweeps")
+        return out
+
+    def status(self):
+        s = ctypes.c_uint()
+        _check(lib.gfc_batch_status(self.h, ctypes.byref(s)), "status")
+        return s.value
+
+    def set_shape(self, minb32=4, minb64=3, round_sweeps=8):
+        _check(lib.gfc_batch_set_shape(self.h, minb32, minb64, round_sweeps), "set_shape")
+
+    @property
+    def kernel_launches(self):
+        return lib.gfc_batch_kernel_launches(self.h)
+
+    @property
+    def stream(self):
+        return lib.gfc_batch_stream(self.h)
+
+    def fix_all(self, params, opts):
+        reports = (Report * self.max_slots)()
+        rounds = lib.gfc_batch_fix_all(self.h, ctypes.byref(params), ctypes.byref(opts), reports)
+        if rounds < 0:
+            raise GFCError(f"gfc_batch_fix_all failed ({rounds}): {last_error()}")
+        return rounds, {s: reports[s] for s in list(self.geom)}

@@ -220,6 +220,69 @@ int  gfc_ctx_get_blocking(const gfc_ctx *c, int *slices64, int *sweeps64, int *s
 #define GFC_NOALLOC_SCRATCH_DOUBLES 16384
 int  gfc_e2_theta_device_noalloc(int ns, int nt, const double *u_dev, void *stream, double *e2, double *theta);
 
+/* ---- batches: many lattices, per-timeslice retirement (no counterpart in the reference) ---- */
+/* A batch holds up to max_slots lattices (even ns, nt <= max_nt, max_sites sites in
+ * total) on one GPU.  Every timeslice of every lattice is swept independently
+ * (timeslices share no link during the sweeps) and retires when its own e2 falls
+ * below the tolerance; with GFC_PREC_MIXED it first runs FP32 bulk sweeps until its
+ * e2 falls below options.switch_e2 and is then rebuilt in FP64.  One round = K
+ * half-sweeps of all active timeslices, replayed as a captured CUDA graph.  Slots
+ * can be added, activated, finalised and removed between rounds (continuous
+ * batching).  Slot memory is allocated stream-ordered (no device synchronisation). */
+typedef struct gfc_batch gfc_batch;
+int    gfc_batch_create(int device, size_t max_sites, int max_slots, int max_nt, gfc_batch **out);
+int    gfc_batch_destroy(gfc_batch *b);
+size_t gfc_batch_slot_bytes(int ns, int nt);          /* device bytes one slot needs */
+int    gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot);   /* GFC_ERR_BUSY when full */
+int    gfc_batch_remove(gfc_batch *b, int slot);
+/* links in (raw reference-layout bytes, as gfc_ctx_upload_links), reunitarised */
+int    gfc_batch_upload(gfc_batch *b, int slot, const void *host, int elem_bytes, int byteswap);
+/* the seeded synthetic configuration of gfc_synth_config built on the device
+ * (same construction and streams; equal to the host one up to rounding), reunitarised */
+int    gfc_batch_synth(gfc_batch *b, int slot, uint64_t seed, double scale);
+/* G = 1; start fixing this slot from the next round (GFC_PREC_MIXED: FP32 first) */
+int    gfc_batch_activate(gfc_batch *b, int slot, int precision);
+/* one round; *active = timeslices still working */
+int    gfc_batch_round(gfc_batch *b, const gfc_params *p, const gfc_options *o, int *active);
+int    gfc_batch_slot_done(gfc_batch *b, int slot, int *done);
+/* retired slot: canonical FP64 links and G, reunitarised, temporal links transformed;
+ * report: sweeps = largest per-timeslice half-sweep count, e2, theta, functional */
+int    gfc_batch_finalize(gfc_batch *b, int slot, gfc_report *r);
+int    gfc_batch_plaquette(gfc_batch *b, int slot, double *spatial, double *temporal);
+int    gfc_batch_download_gt(gfc_batch *b, int slot, void *host, int elem_bytes, int byteswap);
+int    gfc_batch_download_links(gfc_batch *b, int slot, void *host, int elem_bytes, int byteswap);
+int    gfc_batch_status(gfc_batch *b, unsigned *status);
+/* half-sweeps each timeslice of the slot has received (nt ints) */
+int    gfc_batch_slice_sweeps(gfc_batch *b, int slot, int *out);
+long long gfc_batch_kernel_launches(const gfc_batch *b);
+void  *gfc_batch_stream(gfc_batch *b);
+/* minimum resident CTAs per SM of the FP32 / FP64 sweep kernels (1..4) and half-sweeps per round */
+int    gfc_batch_set_shape(gfc_batch *b, int minb32, int minb64, int round_sweeps);
+/* rounds until every activated slot retired (or max_sweeps), then finalise them;
+ * reports indexed by slot; returns the number of rounds */
+int    gfc_batch_fix_all(gfc_batch *b, const gfc_params *p, const gfc_options *o, gfc_report *reports);
+
+/* ---- serving: a request loop with continuous batching (no counterpart in the reference) ---- */
+/* Requests queue on the host; gfc_server_step admits them in arrival order with
+ * first fit while a slot and device memory are free, runs one batch round, and
+ * finalises requests whose timeslices have all retired (G stays resident until
+ * gfc_server_fetch).  Requests join and leave while others are on the GPU; a
+ * request's result does not depend on the others. */
+typedef struct gfc_server gfc_server;
+/* max_sites 0: capacity from mem_fraction of the free device memory */
+int    gfc_server_create(int device, size_t max_sites, double mem_fraction, int max_slots, int max_nt,
+                         gfc_server **out);
+int    gfc_server_destroy(gfc_server *s);
+size_t gfc_server_capacity_sites(const gfc_server *s);
+/* links NULL: the seeded synthetic configuration, built on the device at admission */
+int    gfc_server_submit(gfc_server *s, int ns, int nt, const void *links, int elem_bytes, int byteswap,
+                         uint64_t seed, double scale, int precision, int64_t *id);
+int    gfc_server_step(gfc_server *s, const gfc_params *p, const gfc_options *o, int *running, int *queued);
+/* state 0 queued, 1 running, 2 done, 3 fetched; times are seconds after submit */
+int    gfc_server_poll(gfc_server *s, int64_t id, int *state, double *t_admit, double *t_done, gfc_report *report);
+int    gfc_server_fetch(gfc_server *s, int64_t id, void *gt, int elem_bytes, int release);
+gfc_batch *gfc_server_batch(gfc_server *s);
+
 /* gaugefixOverrelaxation (gauge_fixing.c:713-826) on the resident lattice:
  * sets G = 1, fixes U in place (spatial and temporal links), returns the number of
  * half-sweeps, GFC_FIX_NOT_CONVERGED (-1) or GFC_FIX_BAD_PARAMS (-2); a value below

@@ -1,0 +1,127 @@
+"""The batch engine: many lattices, per-timeslice retirement, graph-replayed rounds.
+
+Properties checked (the batch does not round like the reference, and retires each
+timeslice on its own e2, so parity is stated through what the result must be):
+every lattice ends with e2 below the tolerance, G in SU(3), links equal to
+G U0 G^dagger, plaquettes unchanged to 1e-13, the same gauge functional as a
+single-lattice fix; and a lattice gives bit-identical results alone or admitted
+into a batch that is already running others.
+"""
+import numpy as np
+import pytest
+
+import gfc
+import oracle_ref as orc
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-15
+
+
+def su3_error(G):
+    M = G.reshape(-1, 9, 2)
+    M = (M[..., 0] + 1j * M[..., 1]).reshape(-1, 3, 3)
+    return max(np.abs(M @ M.conj().transpose(0, 2, 1) - np.eye(3)).max(), np.abs(np.linalg.det(M) - 1).max())
+
+
+def params():
+    return gfc.default_params(tolerance=TOL)
+
+
+def test_device_generator_matches_host():
+    ns, nt = 6, 4
+    with gfc.Batch(max_sites=10 ** 5, max_slots=2, max_nt=8) as b:
+        s = b.add(ns, nt)
+        b.synth(s, 81, 0.6)
+        b.activate(s, gfc.PREC_FP64_FAST)
+        b.finalize(s)                # makes the slot readable; links unchanged (no round ran)
+        Ud = b.download_links(s)
+    Uh = gfc.synth_config(ns, nt, 81, 0.6)
+    orc.reunitarize(Uh)
+    np.testing.assert_allclose(Ud, Uh, atol=1e-13)
+
+
+@pytest.mark.parametrize("precision", [gfc.PREC_MIXED, gfc.PREC_FP64_FAST])
+def test_uneven_batch_fixes_every_lattice(precision):
+    geoms = [(4, 8, 71, 0.4), (6, 6, 72, 0.7), (8, 12, 73, 0.5)]
+    U0 = {}
+    with gfc.Batch(max_sites=10 ** 6, max_slots=8, max_nt=16) as b:
+        slots = []
+        for ns, nt, seed, scale in geoms:
+            s = b.add(ns, nt)
+            U = gfc.synth_config(ns, nt, seed, scale)
+            b.upload(s, U, 8, False)
+            orc.reunitarize(U)
+            U0[s] = U
+            slots.append(s)
+        plaq0 = {}
+        for s in slots:
+            b.activate(s, precision)
+        rounds, reps = b.fix_all(params(), gfc.options(precision=precision))
+        assert rounds > 0
+        for s, (ns, nt, seed, scale) in zip(slots, geoms):
+            r = reps[s]
+            assert r.status > 0, r.status
+            assert r.e2 <= 1.5 * TOL
+            G = b.download_gt(s)
+            U = b.download_links(s)
+            assert su3_error(G) < 1e-13
+            U1 = U0[s].copy()
+            orc.apply_gt(U1, G, ns, nt)
+            np.testing.assert_allclose(U1, U, atol=1e-12)
+            for w in (0, 1):
+                assert orc.plaquette(U, ns, nt, w) == pytest.approx(orc.plaquette(U0[s], ns, nt, w), abs=1e-13)
+            # same Coulomb gauge as a single-lattice FP64 fix
+            with gfc.Lattice(ns, nt) as lat:
+                lat.upload_links(U0[s], 8, False)
+                rc, rep1 = lat.fix(params(), gfc.options(precision=gfc.PREC_FP64_FAST, stop_rule=gfc.STOP_EVERY))
+            assert r.functional == pytest.approx(rep1.functional, rel=1e-10)
+            sw = b.slice_sweeps(s)
+            assert sw.min() > 0 and sw.max() == r.sweeps
+        assert b.status() == 0
+
+
+def test_same_result_alone_and_in_the_mix():
+    """Continuous batching: a lattice admitted while others are running gets exactly
+    the result it gets alone."""
+    ns, nt = 6, 8
+    U = gfc.synth_config(ns, nt, 91, 0.5)
+    other = gfc.synth_config(8, 8, 92, 0.6)
+    p, o = params(), gfc.options(precision=gfc.PREC_MIXED)
+    with gfc.Batch(max_sites=10 ** 6, max_slots=4, max_nt=16) as b:
+        s = b.add(ns, nt)
+        b.upload(s, U, 8, False)
+        b.activate(s, gfc.PREC_MIXED)
+        b.fix_all(p, o)
+        G_alone = b.download_gt(s)
+        sw_alone = b.slice_sweeps(s)
+    with gfc.Batch(max_sites=10 ** 6, max_slots=4, max_nt=16) as b:
+        s_other = b.add(8, 8)
+        b.upload(s_other, other, 8, False)
+        b.activate(s_other, gfc.PREC_MIXED)
+        b.round(p, o)
+        b.round(p, o)
+        s = b.add(ns, nt)
+        b.upload(s, U, 8, False)
+        b.activate(s, gfc.PREC_MIXED)
+        active, rounds = 1, 0
+        while active and rounds < 1000:
+            active = b.round(p, o)
+            rounds += 1
+        assert active == 0
+        b.finalize(s)
+        G_mix = b.download_gt(s)
+        assert np.array_equal(b.slice_sweeps(s), sw_alone)
+    assert G_mix.tobytes() == G_alone.tobytes()
+
+
+def test_batch_admission_limits():
+    with gfc.Batch(max_sites=5000, max_slots=2, max_nt=8) as b:
+        with pytest.raises(gfc.GFCError):
+            b.add(5, 4)                  # odd ns
+        with pytest.raises(gfc.GFCError):
+            b.add(4, 16)                 # nt above max_nt
+        s = b.add(8, 8)                  # 4096 sites
+        with pytest.raises(gfc.GFCError):
+            b.add(6, 8)                  # 1728 more: over max_sites
+        b.remove(s)
+        b.add(6, 8)
