@@ -52,6 +52,10 @@ def parse_args():
     p.add_argument("--tol", type=float, default=1e-15)
     p.add_argument("--no-extras", action="store_true", help="skip the mixed/exact comparison runs")
     p.add_argument("--cpu-half-sweeps", type=int, default=8, help="CPU baseline sample per step")
+    p.add_argument("--no-batch", action="store_true", help="skip the 96-config batch run")
+    p.add_argument("--serve-requests", type=int, default=24, help="requests of the serving run (0: skip)")
+    p.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrival rate per second")
+    p.add_argument("--only", default="", help="comma list of batch,serve: run just those (no headline line)")
     return p.parse_args()
 
 
@@ -296,6 +300,123 @@ def run_extras(a, lat, params, stream, torch, gfc, half):
     return res
 
 
+# ----------------------------------------------------- batch and serve --
+BATCH_MIX = [(16, 32)] * 32 + [(24, 48)] * 32 + [(32, 64)] * 32
+SERVE_SIZES = [(16, 32), (24, 48), (32, 64), (48, 96), (64, 128)]
+
+
+def batch_scales(n):
+    """H scales of the batch mix: uniform in [0.3, 0.8], one per config (seeded)."""
+    return np.random.default_rng(100).uniform(0.3, 0.8, n)
+
+
+def site_updates(b, slot, ns, nt):
+    return int(b.slice_sweeps(slot).sum()) * (ns ** 3 // 2)
+
+
+def run_batch(a, gfc, torch, precision):
+    """96 configs of three sizes in one batch: every timeslice retires on its own e2."""
+    mix = BATCH_MIX
+    scales = batch_scales(len(mix))
+    sites = sum(ns ** 3 * nt for ns, nt in mix)
+    b = gfc.Batch(max_sites=sites, max_slots=len(mix), max_nt=max(nt for _, nt in mix))
+    try:
+        stream = torch.cuda.ExternalStream(b.stream)
+        slots = []
+        t0 = time.perf_counter()
+        for k, (ns, nt) in enumerate(mix):
+            s = b.add(ns, nt)
+            b.synth(s, 100 + k, float(scales[k]))
+            slots.append(s)
+        for s in slots:
+            b.activate(s, precision)
+        torch.cuda.synchronize()
+        t_setup = time.perf_counter() - t0
+        params = gfc.default_params(tolerance=a.tol)
+        opts = gfc.options(precision=precision)
+        l0 = b.kernel_launches
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        t0 = time.perf_counter()
+        rounds, reps = b.fix_all(params, opts)
+        ev1.record(stream)
+        ev1.synchronize()
+        wall = time.perf_counter() - t0
+        dev = ev0.elapsed_time(ev1) * 1e-3
+        upd = sum(site_updates(b, s, ns, nt) for s, (ns, nt) in zip(slots, mix))
+        per_size = {}
+        for s, (ns, nt) in zip(slots, mix):
+            sw = b.slice_sweeps(s)
+            d = per_size.setdefault(f"{ns}^3x{nt}", dict(n=0, max_e2=0.0, slice_sweeps_min=1 << 30,
+                                                         slice_sweeps_max=0, not_converged=0))
+            d["n"] += 1
+            d["max_e2"] = max(d["max_e2"], reps[s].e2)
+            d["slice_sweeps_min"] = min(d["slice_sweeps_min"], int(sw.min()))
+            d["slice_sweeps_max"] = max(d["slice_sweeps_max"], int(sw.max()))
+            d["not_converged"] += int(reps[s].status <= 0)
+        return dict(configs=len(mix), sites=sites, seconds=dev, seconds_wall=wall, setup_seconds=t_setup,
+                    rounds=rounds, site_updates=upd, site_updates_per_s=upd / dev, configs_per_s=len(mix) / dev,
+                    kernel_launches=b.kernel_launches - l0, status=b.status(), per_size=per_size,
+                    precision={gfc.PREC_MIXED: "mixed", gfc.PREC_FP64_FAST: "fp64"}[precision])
+    finally:
+        b.close()
+
+
+def serve_requests(n, rate, seed=7):
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    sizes = [SERVE_SIZES[i] for i in rng.integers(0, len(SERVE_SIZES), n)]
+    scales = rng.uniform(0.3, 0.8, n)
+    return [(float(arrivals[i]), sizes[i][0], sizes[i][1], 1000 + i, float(scales[i])) for i in range(n)]
+
+
+def run_serve(a, gfc, precision, n_req, rate):
+    """Poisson stream of requests of mixed sizes through the continuous-batching server.
+
+    Latency runs from a request's arrival time to the moment its G is in host
+    memory and its device memory is released."""
+    reqs = serve_requests(n_req, rate)
+    params = gfc.default_params(tolerance=a.tol)
+    opts = gfc.options(precision=precision)
+    srv = gfc.Server(max_sites=0, mem_fraction=0.85, max_slots=64, max_nt=128)
+    try:
+        cap = srv.capacity_sites
+        pending = list(reqs)
+        live = {}
+        lat, done_t, upd, e2max, rounds = [], [], 0, 0.0, 0
+        t0 = time.perf_counter()
+        while pending or live:
+            now = time.perf_counter() - t0
+            while pending and pending[0][0] <= now:
+                arr, ns, nt, seed, scale = pending.pop(0)
+                rid = srv.submit(ns, nt, seed=seed, scale=scale, precision=precision)
+                live[rid] = (arr, ns, nt)
+            if not live:
+                time.sleep(max(0.0, pending[0][0] - now))
+                continue
+            srv.step(params, opts)
+            rounds += 1
+            for rid in list(live):
+                st, _, _, rep = srv.poll(rid)
+                if st == gfc.REQ_DONE:
+                    srv.fetch(rid)
+                    t = time.perf_counter() - t0
+                    arr, ns, nt = live.pop(rid)
+                    lat.append(t - arr)
+                    done_t.append(t)
+                    upd += rep.site_updates
+                    e2max = max(e2max, rep.e2)
+        span = max(done_t) - reqs[0][0]
+        return dict(requests=n_req, rate_per_s=rate, capacity_sites=cap, rounds=rounds,
+                    p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)),
+                    mean_s=float(np.mean(lat)), configs_per_s=n_req / span, seconds=span,
+                    site_updates_per_s=upd / span, max_e2=e2max,
+                    sizes={f"{ns}^3x{nt}": sum(1 for r in reqs if (r[1], r[2]) == (ns, nt)) for ns, nt in SERVE_SIZES},
+                    precision={gfc.PREC_MIXED: "mixed", gfc.PREC_FP64_FAST: "fp64"}[precision])
+    finally:
+        srv.close()
+
+
 # ------------------------------------------------------- CPU reference --
 def ref_harness():
     has512 = "avx512f" in open("/proc/cpuinfo").read()
@@ -357,7 +478,37 @@ def main():
         rk.close()
         return
 
+    if a.only:
+        import torch
+
+        import gfc
+
+        out = {}
+        for m in a.only.split(","):
+            if m == "batch":
+                out["batch_mixed"] = run_batch(a, gfc, torch, gfc.PREC_MIXED)
+            elif m == "batch64":
+                out["batch_fp64"] = run_batch(a, gfc, torch, gfc.PREC_FP64_FAST)
+            elif m == "serve":
+                out["serve_mixed"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate)
+            elif m == "serve64":
+                out["serve_fp64"] = run_serve(a, gfc, gfc.PREC_FP64_FAST, a.serve_requests, a.serve_rate)
+        if rk.rank == 0:
+            print(json.dumps(out))
+        rk.close()
+        return
+
     r = run_gfc(a, rk)
+    if rk.world == 1:
+        import torch
+
+        import gfc
+
+        if not a.no_batch:
+            r["extras"]["batch_mixed"] = run_batch(a, gfc, torch, gfc.PREC_MIXED)
+        if a.serve_requests > 0:
+            r["extras"]["serve_mixed"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate)
+            r["extras"]["serve_fp64"] = run_serve(a, gfc, gfc.PREC_FP64_FAST, a.serve_requests, a.serve_rate)
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):

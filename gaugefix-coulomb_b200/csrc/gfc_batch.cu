@@ -121,6 +121,8 @@ __global__ void __launch_bounds__(1024) k_compact(BState b) {
         b.counts[1] = min(sc[1][1023], b.cap_items);
         b.counts[2] = min(sc[2][1023], b.cap_pend);
         b.counts[3] = sact[1023];
+        b.counts[6] = 0;
+        b.counts[7] = 0;
     }
 }
 
@@ -136,123 +138,119 @@ __device__ __forceinline__ void slot_fields(const BSlot &sl, typename S::V *&u, 
     }
 }
 
+// Sum of two values over the CTA in a fixed order; the result is valid in thread 0.
+// Leaves the CTA synchronised (the scratch may be reused after it).
+__device__ __forceinline__ void block_pair_sum(double &x, double &y, double (*sh)[BCHUNK / 32]) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_down_sync(0xffffffffu, x, o);
+        y += __shfl_down_sync(0xffffffffu, y, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        sh[0][wid] = x;
+        sh[1][wid] = y;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        x = sh[0][0];
+        y = sh[1][0];
+#pragma unroll
+        for (int q = 1; q < BCHUNK / 32; q++) {
+            x += sh[0][q];
+            y += sh[1][q];
+        }
+    }
+    __syncthreads();
+}
+
 template <class S, int MINB>
 __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
     using T = typename S::T;
-    using C = typename CT<T>::t;
     constexpr bool F64 = sizeof(T) == 8;
     __shared__ double sh[2][BCHUNK / 32];
     __shared__ int last;
+    __shared__ int next[2];
     const int n = b.counts[F64 ? 1 : 0];
     const int k = b.counts[4];
-    const int par = k & 1, op = par ^ 1;
+    const int par = k & 1;
     const int expect = F64 ? SS_FP64 : SS_FP32;
     const int2 *items = F64 ? b.items64 : b.items32;
-    for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    int *cursor = b.counts + (F64 ? 7 : 6);
+    // Items come one at a time from a shared cursor, so a CTA held up by a
+    // timeslice's final reduction does not hold back a fixed share of the list.
+    // Thread 0 asks for item j + 1 while item j is processed and publishes it in
+    // next[(j + 1) & 1] at the end of iteration j; that slot was last read in
+    // iteration j - 1, before the barrier at the top of iteration j.
+    if (threadIdx.x == 0) next[0] = atomicAdd(cursor, 1);
+    for (int j = 0;; j++) {
+        __syncthreads();
+        const int it = next[j & 1];
+        if (it >= n) break;
+        int ahead = 0;
+        if (threadIdx.x == 0) ahead = atomicAdd(cursor, 1);
         const int2 item = items[it];
         const int gid = item.x, chunk = item.y;
-        if (*(volatile int *)&b.state[gid] != expect) continue;   // the same for every thread of the CTA
-        const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
-        const BSlot &sl = b.slots[slot];
-        const Lat l = sl.l;
-        typename S::V *u, *g;
-        slot_fields<S>(sl, u, g);
-        const uint32_t vsh = l.vs >> 1;
-        const uint32_t off = (uint32_t)chunk * BCHUNK + threadIdx.x;
-        double pre = 0.0, post = 0.0;
-        if (off < vsh) {
-            const uint32_t i = (uint32_t)t * vsh + off;
-            Coord c = coord_cb(l, par, i);
-            uint32_t ib[3];
-#pragma unroll
-            for (int d = 0; d < 3; d++) ib[d] = back_L(l, c, d) >> 1;
-            Mt<T> w;
-#pragma unroll
-            for (int q = 0; q < 9; q++) w.e[q] = mkc<C>(T(0), T(0));
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-                Mt<T> f, r;
-                S::load(u + su_idx<S>(l, d, par, i), l.vh, f);
-                S::load(u + su_idx<S>(l, d, op, ib[d]), l.vh, r);
-#pragma unroll
-                for (int x = 0; x < 3; x++)
-#pragma unroll
-                    for (int y = 0; y < 3; y++)
-                        w.e[EL(x, y)] = fadd(w.e[EL(x, y)], fadd(f.e[EL(x, y)], fconj(r.e[EL(y, x)])));
+        // a timeslice retired earlier in this round still has items in the list;
+        // the state is the same for every thread of the CTA
+        if (*(volatile int *)&b.state[gid] == expect) {
+            const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
+            const BSlot &sl = b.slots[slot];
+            const Lat l = sl.l;
+            typename S::V *u, *g;
+            slot_fields<S>(sl, u, g);
+            const uint32_t vsh = l.vs >> 1;
+            const uint32_t off = (uint32_t)chunk * BCHUNK + threadIdx.x;
+            double pre = 0.0, post = 0.0;
+            if (off < vsh) fast_site<S>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, 1, pre, post);
+            // chunk partials (deterministic order inside the block)
+            block_pair_sum(pre, post, sh);
+            if (threadIdx.x == 0) {
+                double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
+                pp[0] = pre;
+                pp[1] = post;
+                __threadfence();
+                last = atomicAdd(&sl.tickets[t], 1u) == (unsigned)sl.nbx - 1;
             }
-            pre = e2_from_w(w);
-            Mt<T> up;
-            fupdate(w, (T)b.omega, b.hits, up);
-            {
-                Mt<T> m, o;
-                S::load(g + sg_idx<S>(l, par, i), l.vh, m);
-                fprod_left<S>(up, m, o);
-                S::store(g + sg_idx<S>(l, par, i), l.vh, o);
-            }
-            double cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-                apply_forward<S>(u + su_idx<S>(l, d, par, i), l.vh, up, 1, cc);
-                apply_backward<S>(u + su_idx<S>(l, d, op, ib[d]), l.vh, up, 1, cc);
-            }
-            cc[7] *= 0.57735026918962576451;
-#pragma unroll
-            for (int q = 0; q < 8; q++) post += cc[q] * cc[q];
-        }
-        // chunk partials (deterministic order inside the block)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            pre += __shfl_down_sync(0xffffffffu, pre, o);
-            post += __shfl_down_sync(0xffffffffu, post, o);
-        }
-        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        if (lane == 0) {
-            sh[0][wid] = pre;
-            sh[1][wid] = post;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double s0 = 0.0, s1 = 0.0;
-            for (int q = 0; q < BCHUNK / 32; q++) {
-                s0 += sh[0][q];
-                s1 += sh[1][q];
-            }
-            double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
-            pp[0] = s0;
-            pp[1] = s1;
-            __threadfence();
-            last = atomicAdd(&sl.tickets[t], 1u) == (unsigned)sl.nbx - 1;
-        }
-        __syncthreads();
-        if (last && threadIdx.x == 0) {
-            double s0 = 0.0, s1 = 0.0;
-            const double *pp = sl.part + (size_t)t * sl.nbx * 2;
-            for (int q = 0; q < sl.nbx; q++) {
-                s0 += __ldcg(pp + 2 * q);
-                s1 += __ldcg(pp + 2 * q + 1);
-            }
-            sl.tickets[t] = 0;
-            double *rprev = b.ring + ((size_t)((k + 1) & 1) * b.nslices + gid) * 2;
-            double *rcur = b.ring + ((size_t)(k & 1) * b.nslices + gid) * 2;
-            const double e2s = (s0 + __ldcg(rprev + 1)) / (double)l.vs;   // e2 of the timeslice after k half-sweeps
-            rcur[0] = s0;
-            rcur[1] = s1;
-            b.sweeps[gid] += 1;
-            if (!(s0 == s0) || !(s1 == s1)) {
-                atomicOr(b.status, GFC_STATUS_NAN);
-                b.state[gid] = SS_DONE;
-            } else if (!F64 && e2s <= b.switch_e2) {
-                b.state[gid] = SS_PEND;
-            } else if (F64 && e2s <= b.tol) {
-                b.state[gid] = SS_DONE;
+            __syncthreads();
+            if (last) {   // uniform: the CTA that completed the timeslice sums its partials
+                double s0 = 0.0, s1 = 0.0;
+                const double *pp = sl.part + (size_t)t * sl.nbx * 2;
+                for (int q = threadIdx.x; q < sl.nbx; q += BCHUNK) {
+                    s0 += __ldcg(pp + 2 * q);
+                    s1 += __ldcg(pp + 2 * q + 1);
+                }
+                block_pair_sum(s0, s1, sh);
+                if (threadIdx.x == 0) {
+                    sl.tickets[t] = 0;
+                    double *rprev = b.ring + ((size_t)((k + 1) & 1) * b.nslices + gid) * 2;
+                    double *rcur = b.ring + ((size_t)(k & 1) * b.nslices + gid) * 2;
+                    // e2 of the timeslice after k half-sweeps
+                    const double e2s = (s0 + __ldcg(rprev + 1)) / (double)l.vs;
+                    rcur[0] = s0;
+                    rcur[1] = s1;
+                    b.sweeps[gid] += 1;
+                    if (!(s0 == s0) || !(s1 == s1)) {
+                        atomicOr(b.status, GFC_STATUS_NAN);
+                        b.state[gid] = SS_DONE;
+                    } else if (!F64 && e2s <= b.switch_e2) {
+                        b.state[gid] = SS_PEND;
+                    } else if (F64 && e2s <= b.tol) {
+                        b.state[gid] = SS_DONE;
+                    }
+                }
             }
         }
-        __syncthreads();
+        if (threadIdx.x == 0) next[(j + 1) & 1] = ahead;
     }
 }
 
 __global__ void k_btick(BState b) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) b.counts[4] += 1;
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        b.counts[4] += 1;
+        b.counts[6] = 0;   // item cursors of the next half-sweep
+        b.counts[7] = 0;
+    }
 }
 
 // projectSU3 of a timeslice's working fields after every `period` of its own
@@ -399,7 +397,7 @@ struct gfc_batch {
     cudaGraphExec_t exec = nullptr;
     int round_k = 8;
     BState captured{};
-    int grid = 0;
+    int grid = 0, nsm = 0;
     int minb32 = 4, minb64 = 3;
     long long launches = 0;
     long long rounds = 0;
@@ -455,7 +453,8 @@ extern "C" int gfc_batch_create(int device, size_t max_sites, int max_slots, int
     {
         int nsm = 0;
         BTRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-        b->grid = nsm * 4;   // persistent CTAs; more than resident is harmless (they loop)
+        b->nsm = nsm;
+        b->grid = nsm * 4;   // persistent CTAs of the reunit / switch kernels (they loop)
     }
 #undef BTRY
     *out = b;
@@ -712,8 +711,10 @@ static void enqueue_round(gfc_batch *b, const BState &bs) {
     k_switch_u<<<b->grid, BCHUNK, 0, st>>>(bs);
     k_switch_done<<<(b->nslices + 255) / 256, 256, 0, st>>>(bs);
     for (int k = 0; k < b->round_k; k++) {
-        launch_bsweep<S32>(b->minb32, b->grid, st, bs);
-        launch_bsweep<S64R>(b->minb64, b->grid, st, bs);
+        // one resident wave of persistent CTAs: a CTA that had to wait for a slot
+        // would start its share of the items late and stretch the tail
+        launch_bsweep<S32>(b->minb32, b->nsm * b->minb32, st, bs);
+        launch_bsweep<S64R>(b->minb64, b->nsm * b->minb64, st, bs);
         k_btick<<<1, 32, 0, st>>>(bs);
         k_breunit<S32><<<b->grid, BCHUNK, 0, st>>>(bs, bs.reunit32);
         k_breunit<S64R><<<b->grid, BCHUNK, 0, st>>>(bs, bs.reunit64);

@@ -113,36 +113,43 @@ __device__ void fused_reduce(const SweepArgs &a, double pre, double post) {
     }
     __syncthreads();
     if (!last) return;
-    // slice sum in index order
-    if (threadIdx.x == 0) {
-        double s0 = 0.0, s1 = 0.0;
+    // slice sum: each thread a fixed strided share of the partials, then the block
+    // tree (a fixed order, so the result does not depend on which block came last)
+    {
         const double *p = a.part + (size_t)t * nbx * 2;
-        for (uint32_t b = 0; b < nbx; b++) {
-            s0 += __ldcg(p + 2 * b);
-            s1 += __ldcg(p + 2 * b + 1);
+        v[0] = v[1] = 0.0;
+        for (uint32_t b = threadIdx.x; b < nbx; b += BLOCK) {
+            v[0] += __ldcg(p + 2 * b);
+            v[1] += __ldcg(p + 2 * b + 1);
         }
+        fblock_sum<BLOCK, 2>(v, sh);
+    }
+    if (threadIdx.x == 0) {
         a.tickets[t] = 0;
         if (a.track == 2) {
             // slice-blocked sweeping: the whole-lattice test runs after the round
             double *r = a.ring + ((size_t)(a.sweep % a.ring_n) * a.l.nt + t) * 2;
-            r[0] = s0;
-            r[1] = s1;
+            r[0] = v[0];
+            r[1] = v[1];
             last = 0;
         } else {
-            a.slice[2 * t] = s0;
-            a.slice[2 * t + 1] = s1;
+            a.slice[2 * t] = v[0];
+            a.slice[2 * t + 1] = v[1];
             __threadfence();
             unsigned tk = atomicAdd(&a.tickets[nt], 1u);
             last = tk == nt - 1;
         }
     }
     __syncthreads();
-    if (!last || threadIdx.x != 0) return;
-    double s0 = 0.0, s1 = 0.0;
-    for (uint32_t q = 0; q < nt; q++) {
-        s0 += __ldcg(a.slice + 2 * q);
-        s1 += __ldcg(a.slice + 2 * q + 1);
+    if (!last) return;
+    v[0] = v[1] = 0.0;
+    for (uint32_t q = threadIdx.x; q < nt; q += BLOCK) {
+        v[0] += __ldcg(a.slice + 2 * q);
+        v[1] += __ldcg(a.slice + 2 * q + 1);
     }
+    fblock_sum<BLOCK, 2>(v, sh);
+    if (threadIdx.x != 0) return;
+    const double s0 = v[0], s1 = v[1];
     a.tickets[nt] = 0;
     if (a.sweep < a.hist_n) {
         a.hist[2 * a.sweep] = s0;
@@ -163,60 +170,13 @@ template <class S, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_fast(typename S::V *__restrict__ u,
                                                             typename S::V *__restrict__ g, SweepArgs a) {
     using T = typename S::T;
-    using C = typename CT<T>::t;
     if (a.stop && *(volatile unsigned *)a.stop) return;
     const Lat &l = a.l;
     const uint32_t vsh = l.vs >> 1;
     const uint32_t off = blockIdx.x * BLOCK + threadIdx.x;
     const bool active = off < vsh;
     double pre = 0.0, post = 0.0;
-    if (active) {
-        const int par = a.par, op = par ^ 1;
-        const uint32_t i = (a.t0 + blockIdx.y) * vsh + off;
-        Coord c = coord_cb(l, par, i);
-        uint32_t ib[3];
-#pragma unroll
-        for (int d = 0; d < 3; d++) ib[d] = back_L(l, c, d) >> 1;
-
-        Mt<T> w;
-#pragma unroll
-        for (int k = 0; k < 9; k++) w.e[k] = mkc<C>(T(0), T(0));
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            Mt<T> f, r;
-            S::load(u + su_idx<S>(l, d, par, i), l.vh, f);
-            S::load(u + su_idx<S>(l, d, op, ib[d]), l.vh, r);
-#pragma unroll
-            for (int x = 0; x < 3; x++)
-#pragma unroll
-                for (int y = 0; y < 3; y++) w.e[EL(x, y)] = fadd(w.e[EL(x, y)], fadd(f.e[EL(x, y)], fconj(r.e[EL(y, x)])));
-        }
-        if (a.track) pre = e2_from_w(w);
-
-        Mt<T> up;
-        fupdate(w, (T)a.omega, a.hits, up);
-
-        // G(x) <- up G(x)
-        {
-            Mt<T> m, o;
-            S::load(g + sg_idx<S>(l, par, i), l.vh, m);
-            fprod_left<S>(up, m, o);
-            S::store(g + sg_idx<S>(l, par, i), l.vh, o);
-        }
-        // links; the post-update w(x) enters e2 only through its 8 algebra
-        // components, accumulated row by row (see acc_row)
-        double cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            apply_forward<S>(u + su_idx<S>(l, d, par, i), l.vh, up, a.track, cc);
-            apply_backward<S>(u + su_idx<S>(l, d, op, ib[d]), l.vh, up, a.track, cc);
-        }
-        if (a.track) {
-            cc[7] *= 0.57735026918962576451;
-#pragma unroll
-            for (int k = 0; k < 8; k++) post += cc[k] * cc[k];
-        }
-    }
+    if (active) fast_site<S>(u, g, l, a.par, (a.t0 + blockIdx.y) * vsh + off, (T)a.omega, a.hits, a.track, pre, post);
     if (a.track) fused_reduce<BLOCK>(a, pre, post);
 }
 

@@ -411,4 +411,62 @@ __device__ __forceinline__ void apply_backward(typename S::V *__restrict__ p, si
     }
 }
 
+// One site of a checkerboard half-sweep: w(x) from the three forward and three
+// backward spatial links, the over-relaxed SU(3) update, G(x) <- up G(x) and the six
+// links updated in place.  pre / post receive the site's contributions to e2 before
+// and after the update (when track != 0).  u and g do not alias: with that known the
+// compiler keeps the links it loaded for w(x) in registers for the link update
+// instead of loading them again after the store to G.
+template <class S>
+__device__ __forceinline__ void fast_site(typename S::V *__restrict__ u, typename S::V *__restrict__ g,
+                                          const Lat &l, int par, uint32_t i, typename S::T omega,
+                                          unsigned hits, int track, double &pre, double &post) {
+    using T = typename S::T;
+    using C = typename CT<T>::t;
+    const int op = par ^ 1;
+    Coord c = coord_cb(l, par, i);
+    uint32_t ib[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) ib[d] = back_L(l, c, d) >> 1;
+
+    Mt<T> w;
+#pragma unroll
+    for (int k = 0; k < 9; k++) w.e[k] = mkc<C>(T(0), T(0));
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        Mt<T> f, r;
+        S::load(u + su_idx<S>(l, d, par, i), l.vh, f);
+        S::load(u + su_idx<S>(l, d, op, ib[d]), l.vh, r);
+#pragma unroll
+        for (int x = 0; x < 3; x++)
+#pragma unroll
+            for (int y = 0; y < 3; y++) w.e[EL(x, y)] = fadd(w.e[EL(x, y)], fadd(f.e[EL(x, y)], fconj(r.e[EL(y, x)])));
+    }
+    if (track) pre = e2_from_w(w);
+
+    Mt<T> up;
+    fupdate(w, omega, hits, up);
+
+    // G(x) <- up G(x)
+    {
+        Mt<T> m, o;
+        S::load(g + sg_idx<S>(l, par, i), l.vh, m);
+        fprod_left<S>(up, m, o);
+        S::store(g + sg_idx<S>(l, par, i), l.vh, o);
+    }
+    // links; the post-update w(x) enters e2 only through its 8 algebra components,
+    // accumulated row by row (acc_row)
+    double cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        apply_forward<S>(u + su_idx<S>(l, d, par, i), l.vh, up, track, cc);
+        apply_backward<S>(u + su_idx<S>(l, d, op, ib[d]), l.vh, up, track, cc);
+    }
+    if (track) {
+        cc[7] *= 0.57735026918962576451;
+#pragma unroll
+        for (int k = 0; k < 8; k++) post += cc[k] * cc[k];
+    }
+}
+
 }  // namespace gfc

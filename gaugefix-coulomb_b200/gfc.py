@@ -510,3 +510,100 @@ class Batch:
         if rounds < 0:
             raise GFCError(f"gfc_batch_fix_all failed ({rounds}): {last_error()}")
         return rounds, {s: reports[s] for s in list(self.geom)}
+
+
+def _bind_server():
+    P, I, D, S = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+    IP, DP = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "gfc_server_create": (I, [I, S, D, I, I, ctypes.POINTER(P)]),
+        "gfc_server_destroy": (I, [P]),
+        "gfc_server_capacity_sites": (S, [P]),
+        "gfc_server_submit": (I, [P, I, I, P, I, I, ctypes.c_uint64, D, I, ctypes.POINTER(ctypes.c_int64)]),
+        "gfc_server_step": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), IP, IP]),
+        "gfc_server_poll": (I, [P, ctypes.c_int64, IP, DP, DP, ctypes.POINTER(Report)]),
+        "gfc_server_fetch": (I, [P, ctypes.c_int64, P, I, I]),
+        "gfc_server_batch": (P, [P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+
+
+_bind_server()
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FETCHED = 0, 1, 2, 3
+
+
+class Server:
+    """Request loop with continuous batching over one Batch (a gfc_server).
+
+    submit() queues a lattice; step() admits what fits in free device memory,
+    runs one round and finalises finished requests; fetch() returns G and frees
+    the request's device memory."""
+
+    def __init__(self, max_sites=0, mem_fraction=0.85, max_slots=256, max_nt=128, device=0):
+        h = ctypes.c_void_p()
+        _check(lib.gfc_server_create(device, int(max_sites), mem_fraction, max_slots, max_nt, ctypes.byref(h)),
+               "gfc_server_create")
+        self.h = h
+        self.geom = {}
+
+    def close(self):
+        if self.h:
+            lib.gfc_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def capacity_sites(self):
+        return lib.gfc_server_capacity_sites(self.h)
+
+    def submit(self, ns, nt, links=None, elem_bytes=8, byteswap=False, seed=0, scale=0.5, precision=PREC_MIXED):
+        rid = ctypes.c_int64()
+        ptr = None
+        if links is not None:
+            links = np.ascontiguousarray(links)
+            assert links.nbytes == ns ** 3 * nt * 4 * 18 * elem_bytes
+            ptr = links.ctypes.data
+        _check(lib.gfc_server_submit(self.h, ns, nt, ptr, elem_bytes, int(byteswap), seed, scale, precision,
+                                     ctypes.byref(rid)), "gfc_server_submit")
+        self.geom[rid.value] = (ns, nt)
+        return rid.value
+
+    def step(self, params, opts):
+        r, q = ctypes.c_int(), ctypes.c_int()
+        _check(lib.gfc_server_step(self.h, ctypes.byref(params), ctypes.byref(opts), ctypes.byref(r),
+                                   ctypes.byref(q)), "gfc_server_step")
+        return r.value, q.value
+
+    def poll(self, rid):
+        st, ta, td = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+        rep = Report()
+        _check(lib.gfc_server_poll(self.h, rid, ctypes.byref(st), ctypes.byref(ta), ctypes.byref(td),
+                                   ctypes.byref(rep)), "gfc_server_poll")
+        return st.value, ta.value, td.value, rep
+
+    def fetch(self, rid, elem_bytes=8, release=True, want_gt=True):
+        out = None
+        if want_gt:
+            ns, nt = self.geom[rid]
+            out = np.empty(ns ** 3 * nt * 18, dtype=np.float64 if elem_bytes == 8 else np.float32)
+        _check(lib.gfc_server_fetch(self.h, rid, None if out is None else out.ctypes.data, elem_bytes,
+                                    int(release)), "gfc_server_fetch")
+        return out
+
+    def batch_stream(self):
+        return lib.gfc_batch_stream(lib.gfc_server_batch(self.h))
+
+    def kernel_launches(self):
+        return lib.gfc_batch_kernel_launches(lib.gfc_server_batch(self.h))
