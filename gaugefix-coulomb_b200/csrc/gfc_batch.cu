@@ -260,33 +260,46 @@ template <class S>
 __global__ void __launch_bounds__(BCHUNK) k_breunit(BState b, unsigned period) {
     constexpr bool F64 = sizeof(typename S::T) == 8;
     if (period == 0) return;
+    __shared__ int due[BCHUNK];
+    __shared__ int ndue;
     const int n = b.counts[F64 ? 1 : 0];
     const int2 *items = F64 ? b.items64 : b.items32;
     const int expect = F64 ? SS_FP64 : SS_FP32;
-    for (int it = blockIdx.x; it < n; it += gridDim.x) {
-        const int2 item = items[it];
-        const int gid = item.x;
-        if (*(volatile int *)&b.state[gid] != expect) continue;
-        const int own = b.sweeps[gid];
-        if (own == 0 || (unsigned)own % period) continue;
-        const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
-        const BSlot &sl = b.slots[slot];
-        const Lat l = sl.l;
-        typename S::V *u, *g;
-        slot_fields<S>(sl, u, g);
-        const uint32_t vsh = l.vs >> 1;
-        const uint32_t off = (uint32_t)item.y * BCHUNK + threadIdx.x;
-        if (off >= vsh) continue;
-        const uint32_t i = (uint32_t)t * vsh + off;
-        for (int par = 0; par < 2; par++) {
-            for (int d = 0; d <= 3; d++) {
-                typename S::V *p = d < 3 ? u + su_idx<S>(l, d, par, i) : g + sg_idx<S>(l, par, i);
-                Mt<typename S::T> m;
-                S::load(p, l.vh, m);
-                if (!fproject(m)) atomicOr(b.status, GFC_STATUS_PROJECT_FAIL);
-                S::store(p, l.vh, m);
+    // the CTA examines BCHUNK items at once (one per thread) and projects only the
+    // chunks of timeslices that are due; most half-sweeps none are
+    for (int base = blockIdx.x * BCHUNK; base < n; base += gridDim.x * BCHUNK) {
+        if (threadIdx.x == 0) ndue = 0;
+        __syncthreads();
+        const int it = base + threadIdx.x;
+        if (it < n) {
+            const int gid = items[it].x;
+            const int own = b.sweeps[gid];
+            if (b.state[gid] == expect && own != 0 && (unsigned)own % period == 0) due[atomicAdd(&ndue, 1)] = it;
+        }
+        __syncthreads();
+        for (int q = 0; q < ndue; q++) {   // independent chunks: their order does not matter
+            const int2 item = items[due[q]];
+            const int gid = item.x;
+            const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
+            const BSlot &sl = b.slots[slot];
+            const Lat l = sl.l;
+            typename S::V *u, *g;
+            slot_fields<S>(sl, u, g);
+            const uint32_t vsh = l.vs >> 1;
+            const uint32_t off = (uint32_t)item.y * BCHUNK + threadIdx.x;
+            if (off >= vsh) continue;
+            const uint32_t i = (uint32_t)t * vsh + off;
+            for (int par = 0; par < 2; par++) {
+                for (int d = 0; d <= 3; d++) {
+                    typename S::V *p = d < 3 ? u + su_idx<S>(l, d, par, i) : g + sg_idx<S>(l, par, i);
+                    Mt<typename S::T> m;
+                    S::load(p, l.vh, m);
+                    if (!fproject(m)) atomicOr(b.status, GFC_STATUS_PROJECT_FAIL);
+                    S::store(p, l.vh, m);
+                }
             }
         }
+        __syncthreads();
     }
 }
 
@@ -399,6 +412,9 @@ struct gfc_batch {
     BState captured{};
     int grid = 0, nsm = 0;
     int minb32 = 4, minb64 = 3;
+    // slot memory: a pool of its own that keeps freed memory mapped, so a slot
+    // freed and another admitted costs no unmapping and remapping of device memory
+    cudaMemPool_t pool = nullptr;
     long long launches = 0;
     long long rounds = 0;
 };
@@ -449,6 +465,15 @@ extern "C" int gfc_batch_create(int device, size_t max_sites, int max_slots, int
     BTRY(cudaMallocHost(&b->hcounts, sizeof(int) * 8));
     BTRY(cudaMallocHost(&b->hstate, sizeof(int) * b->nslices));
     BTRY(cudaMalloc(&b->dres, sizeof(double) * 8));
+    {
+        cudaMemPoolProps pp{};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = device;
+        BTRY(cudaMemPoolCreate(&b->pool, &pp));
+        uint64_t keep = UINT64_MAX;
+        BTRY(cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     BTRY(cudaMallocHost(&b->hres, sizeof(double) * 8));
     {
         int nsm = 0;
@@ -471,7 +496,9 @@ extern "C" int gfc_batch_destroy(gfc_batch *b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     for (void *m : b->mem)
-        if (m) cudaFree(m);
+        if (m) cudaFreeAsync(m, b->s);
+    cudaStreamSynchronize(b->s);
+    if (b->pool) cudaMemPoolDestroy(b->pool);
     cudaFree(b->dslots);
     cudaFree(b->state);
     cudaFree(b->sweeps);
@@ -528,7 +555,14 @@ extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
     GFC_CHECK(cudaSetDevice(b->dev));
     const size_t bytes = gfc_batch_slot_bytes(ns, nt);
     void *m = nullptr;
-    cudaError_t e = cudaMallocAsync(&m, bytes, b->s);
+    cudaError_t e = cudaMallocFromPoolAsync(&m, bytes, b->pool, b->s);
+    if (e != cudaSuccess) {
+        // memory kept by the pool may be split badly for this size: return it and retry
+        cudaGetLastError();
+        GFC_CHECK(cudaStreamSynchronize(b->s));
+        GFC_CHECK(cudaMemPoolTrimTo(b->pool, 0));
+        e = cudaMallocFromPoolAsync(&m, bytes, b->pool, b->s);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         set_error("device memory for a %d^3x%d slot (%zu bytes): %s", ns, nt, bytes, cudaGetErrorString(e));
@@ -821,6 +855,8 @@ extern "C" int gfc_batch_finalize(gfc_batch *b, int slot, gfc_report *r) {
         r->functional = b->hres[2] / ((double)l.v * 9.0);
         r->final_residue = r->e2;
         r->status = mx;
+    } else {
+        GFC_CHECK(cudaStreamSynchronize(b->s));   // a copy on another stream may follow
     }
     GFC_CHECK(cudaGetLastError());
     b->activated[slot] = 0;
@@ -840,7 +876,10 @@ extern "C" int gfc_batch_plaquette(gfc_batch *b, int slot, double *spatial, doub
     return GFC_OK;
 }
 
-extern "C" int gfc_batch_download_gt(gfc_batch *b, int slot, void *host, int elem_bytes, int byteswap) {
+namespace gfc {
+// G of a finalised slot to host memory on stream `st` (the caller's stream: the
+// request server downloads on its own stream while rounds run on the batch's)
+int batch_download_gt_on(gfc_batch *b, int slot, void *host, int elem_bytes, int byteswap, cudaStream_t st) {
     int rc = check_slot(b, slot);
     if (rc) return rc;
     if (b->activated[slot]) {
@@ -858,12 +897,33 @@ extern "C" int gfc_batch_download_gt(gfc_batch *b, int slot, void *host, int ele
     const uint32_t per = (uint32_t)std::max<size_t>(1, stage / per_slice);
     for (uint32_t t0 = 0; t0 < (uint32_t)l.nt; t0 += per) {
         uint32_t n = std::min<uint32_t>(per, l.nt - t0);
-        launch_store_gt(sl.g, l, t0, n, elem_bytes, byteswap, sl.u64r, b->s);
+        launch_store_gt(sl.g, l, t0, n, elem_bytes, byteswap, sl.u64r, st);
         GFC_CHECK(cudaMemcpyAsync((char *)host + (size_t)t0 * per_slice, sl.u64r, n * per_slice,
-                                  cudaMemcpyDeviceToHost, b->s));
+                                  cudaMemcpyDeviceToHost, st));
     }
+    GFC_CHECK(cudaStreamSynchronize(st));
+    return GFC_OK;
+}
+
+// Map `bytes` of device memory into the slot pool ahead of time (allocated and
+// freed once; the pool keeps it), so admissions do not wait for the mapping.
+int batch_warm_pool(gfc_batch *b, size_t bytes) {
+    GFC_CHECK(cudaSetDevice(b->dev));
+    void *m = nullptr;
+    if (cudaMallocFromPoolAsync(&m, bytes, b->pool, b->s) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cannot map %zu bytes of device memory for the slot pool", bytes);
+        return GFC_ERR_NOMEM;
+    }
+    GFC_CHECK(cudaFreeAsync(m, b->s));
     GFC_CHECK(cudaStreamSynchronize(b->s));
     return GFC_OK;
+}
+}  // namespace gfc
+
+extern "C" int gfc_batch_download_gt(gfc_batch *b, int slot, void *host, int elem_bytes, int byteswap) {
+    if (!b) return GFC_ERR_ARG;
+    return batch_download_gt_on(b, slot, host, elem_bytes, byteswap, b->s);
 }
 
 extern "C" int gfc_batch_download_links(gfc_batch *b, int slot, void *host, int elem_bytes, int byteswap) {

@@ -10,6 +10,8 @@
 #define GFC_STATUS_NAN          2u   // a reduction produced NaN
 #define GFC_STATUS_CONVERGED    4u   // a device-side stopping test fired
 
+struct gfc_batch;
+
 namespace gfc {
 
 // ---- exact FP64 kernels (gfc_kernels_exact.cu)
@@ -52,5 +54,11 @@ void launch_synth(const Lat &l, uint64_t seed, double scale, double2 *gtmp, doub
 // plaquette partials: [nt][nbx][2] = (spatial sum, temporal sum) of Re Tr/3
 void launch_plaquette(const double2 *u, const double2 *ut, const Lat &l, double *part, double *out,
                       cudaStream_t s);
+
+// ---- batch internals shared with the request server (gfc_batch.cu)
+// G of a finalised slot to host memory, staged and copied on stream st; synchronous
+int batch_download_gt_on(::gfc_batch *b, int slot, void *host, int elem_bytes, int byteswap, cudaStream_t st);
+// map `bytes` of device memory into the batch's slot pool ahead of time
+int batch_warm_pool(::gfc_batch *b, size_t bytes);
 
 }  // namespace gfc

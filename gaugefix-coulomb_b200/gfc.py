@@ -523,7 +523,11 @@ def _bind_server():
         "gfc_server_step": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), IP, IP]),
         "gfc_server_poll": (I, [P, ctypes.c_int64, IP, DP, DP, ctypes.POINTER(Report)]),
         "gfc_server_fetch": (I, [P, ctypes.c_int64, P, I, I]),
+        "gfc_server_result": (I, [P, ctypes.c_int64, ctypes.POINTER(ctypes.POINTER(ctypes.c_double)),
+                                  ctypes.POINTER(ctypes.c_size_t)]),
         "gfc_server_batch": (P, [P]),
+        "gfc_server_reserve_host": (I, [P, S, I]),
+        "gfc_server_stats": (I, [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -601,6 +605,28 @@ class Server:
         _check(lib.gfc_server_fetch(self.h, rid, None if out is None else out.ctypes.data, elem_bytes,
                                     int(release)), "gfc_server_fetch")
         return out
+
+    def result_view(self, rid):
+        """G of a done request as a read-only view of the server's host copy
+        (valid until fetch(..., release=True))."""
+        p, n = ctypes.POINTER(ctypes.c_double)(), ctypes.c_size_t()
+        _check(lib.gfc_server_result(self.h, rid, ctypes.byref(p), ctypes.byref(n)), "gfc_server_result")
+        a = np.ctypeslib.as_array(p, shape=(n.value,))
+        a.flags.writeable = False
+        return a
+
+    def reserve_host(self, buffer_bytes, count):
+        """Pin host result buffers ahead of time."""
+        _check(lib.gfc_server_reserve_host(self.h, int(buffer_bytes), count), "gfc_server_reserve_host")
+
+    def stats(self):
+        """Host seconds per phase of step() and the rounds run."""
+        sec, n = (ctypes.c_double * 4)(), ctypes.c_longlong()
+        _check(lib.gfc_server_stats(self.h, sec, ctypes.byref(n)), "gfc_server_stats")
+        return dict(release_s=sec[0], admission_s=sec[1], rounds_s=sec[2], finalize_s=sec[3], rounds=n.value)
+
+    def release(self, rid):
+        _check(lib.gfc_server_fetch(self.h, rid, None, 8, 1), "gfc_server_fetch")
 
     def batch_stream(self):
         return lib.gfc_batch_stream(lib.gfc_server_batch(self.h))

@@ -263,11 +263,13 @@ int    gfc_batch_set_shape(gfc_batch *b, int minb32, int minb64, int round_sweep
 int    gfc_batch_fix_all(gfc_batch *b, const gfc_params *p, const gfc_options *o, gfc_report *reports);
 
 /* ---- serving: a request loop with continuous batching (no counterpart in the reference) ---- */
-/* Requests queue on the host; gfc_server_step admits them in arrival order with
- * first fit while a slot and device memory are free, runs one batch round, and
- * finalises requests whose timeslices have all retired (G stays resident until
- * gfc_server_fetch).  Requests join and leave while others are on the GPU; a
- * request's result does not depend on the others. */
+/* Requests queue on the host; gfc_server_step releases the device memory of
+ * requests whose G has reached the host, admits queued requests in arrival order
+ * with first fit while a slot and device memory are free, runs one batch round and
+ * finalises requests whose timeslices have all retired.  A result thread copies
+ * each finished G to host memory on its own stream while the next rounds run.
+ * Requests join and leave while others are on the GPU; a request's result does
+ * not depend on the others.  The gfc_server_* calls are made from one thread. */
 typedef struct gfc_server gfc_server;
 /* max_sites 0: capacity from mem_fraction of the free device memory */
 int    gfc_server_create(int device, size_t max_sites, double mem_fraction, int max_slots, int max_nt,
@@ -278,9 +280,19 @@ size_t gfc_server_capacity_sites(const gfc_server *s);
 int    gfc_server_submit(gfc_server *s, int ns, int nt, const void *links, int elem_bytes, int byteswap,
                          uint64_t seed, double scale, int precision, int64_t *id);
 int    gfc_server_step(gfc_server *s, const gfc_params *p, const gfc_options *o, int *running, int *queued);
-/* state 0 queued, 1 running, 2 done, 3 fetched; times are seconds after submit */
+/* state 0 queued, 1 running (or G on its way to the host), 2 done (G on the host),
+ * 3 fetched; times are seconds after submit */
 int    gfc_server_poll(gfc_server *s, int64_t id, int *state, double *t_admit, double *t_done, gfc_report *report);
+/* G of a done request (reference layout, FP64) in place: valid until released */
+int    gfc_server_result(gfc_server *s, int64_t id, const double **gt, size_t *count);
+/* copy G (elem_bytes 8 or 4; gt may be NULL) and, with release != 0, drop the host copy */
 int    gfc_server_fetch(gfc_server *s, int64_t id, void *gt, int elem_bytes, int release);
+/* pin `count` host buffers of `buffer_bytes` for results ahead of time (results
+ * go to reused page-locked buffers, up to 32 GiB of them) */
+int    gfc_server_reserve_host(gfc_server *s, size_t buffer_bytes, int count);
+/* host seconds in the phases of gfc_server_step (release, admission, rounds,
+ * finalisation) and the rounds run */
+int    gfc_server_stats(const gfc_server *s, double *seconds4, long long *rounds);
 gfc_batch *gfc_server_batch(gfc_server *s);
 
 /* gaugefixOverrelaxation (gauge_fixing.c:713-826) on the resident lattice:
