@@ -53,6 +53,7 @@ def parse_args():
     p.add_argument("--no-extras", action="store_true", help="skip the mixed/exact comparison runs")
     p.add_argument("--cpu-half-sweeps", type=int, default=8, help="CPU baseline sample per step")
     p.add_argument("--no-batch", action="store_true", help="skip the 96-config batch run")
+    p.add_argument("--no-precision-form", action="store_true", help="skip the 48^3x96 FP32-input mixed run")
     p.add_argument("--serve-requests", type=int, default=24, help="requests of the serving run (0: skip)")
     p.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrival rate per second")
     p.add_argument("--only", default="", help="comma list of batch,serve: run just those (no headline line)")
@@ -61,7 +62,11 @@ def parse_args():
 
 # ----------------------------------------------------------------- ranks --
 class Ranks:
-    def __init__(self):
+    """One process per GPU (torchrun environment).  Each rank fixes its own replica;
+    the only collectives are the barrier around the timed region and the reduction
+    of timing scalars.  NCCL with GPUs, gloo without (the CPU tests of this logic)."""
+
+    def __init__(self, backend=None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -72,9 +77,13 @@ class Ranks:
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            cuda = torch.cuda.is_available() and backend != "gloo"
+            if cuda:
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend or ("nccl" if cuda else "gloo"),
+                                    timeout=datetime.timedelta(seconds=300))
             self.dist, self.torch = dist, torch
+            self.device = f"cuda:{self.local}" if cuda else "cpu"
 
     def barrier(self):
         if self.dist:
@@ -83,9 +92,15 @@ class Ranks:
     def reduce(self, x, op):
         if not self.dist:
             return x
-        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device="cuda")
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t, op=getattr(self.dist.ReduceOp, op))
         return t.item()
+
+    def aggregate(self, seconds, units):
+        """Whole-job throughput: units of all ranks over the slowest rank's time."""
+        t = self.reduce(seconds, "MAX")
+        n = self.reduce(units, "SUM")
+        return t, n, n / t
 
     def close(self):
         if self.dist:
@@ -197,11 +212,8 @@ def run_gfc(a, rk):
     launches = lat.kernel_launches - l0
     clk = clocks.stop()
     elapsed = ev0.elapsed_time(ev1) * 1e-3
-    elapsed_max = rk.reduce(elapsed, "MAX")
     sweeps = [r.sweeps for r in reps]
-    updates = sum(sweeps) * half
-    updates_all = rk.reduce(updates, "SUM")
-    value = updates_all / elapsed_max
+    elapsed_max, updates_all, value = rk.aggregate(elapsed, sum(sweeps) * half)
     # dominant kernel: the FP64 half-sweep; its average duration inside the fix
     # loop (CUDA events on the launching stream, includes the periodic reunit)
     loop_s = sum(r.seconds_sweeps for r in reps)
@@ -221,8 +233,7 @@ def run_gfc(a, rk):
         t1 = time.perf_counter()
         if k >= a.warmup:
             e2e_t.append((t1 - t0, rep.sweeps))
-    e2e_time = rk.reduce(sum(t for t, _ in e2e_t), "MAX")
-    e2e_updates = rk.reduce(sum(s for _, s in e2e_t) * half, "SUM")
+    e2e_time, e2e_updates, _ = rk.aggregate(sum(t for t, _ in e2e_t), sum(s for _, s in e2e_t) * half)
     lat.restore_links()
 
     extras = {}
@@ -297,6 +308,49 @@ def run_extras(a, lat, params, stream, torch, gfc, half):
     lat.restore_links()
     res["kernel_fp64_exact_s"] = timed_halfsweeps(lat, stream, torch, 32, gfc.PREC_FP64_EXACT)
     lat.restore_links()
+    return res
+
+
+def run_precision_form(a, gfc):
+    """48^3x96, H scale 0.7, seed 3, stored FP32 (big endian) and converted on load:
+    mixed FP32 bulk / FP64 refinement (reunitarised every 10 FP64 half-sweeps) beside
+    the FP64 paths on the same input.  The reference-arithmetic FP64 path (bit for bit
+    the reference's update) stands in for the FP64 oracle at this size."""
+    ns, nt, seed, scale = 48, 96, 3, 0.7
+    U = gfc.synth_config(ns, nt, seed, scale)
+    raw = gfc.PinnedBuffer(U.size * 4)
+    raw.view(">f4")[:] = U
+    del U
+    params = gfc.default_params(tolerance=a.tol)
+    res = {"lattice": [ns, nt], "seed": seed, "h_scale": scale, "input": "FP32 big endian, converted on load"}
+    with gfc.Lattice(ns, nt, mixed=True) as lat:
+        lat.upload_links(raw.array, 4, byteswap=True)
+        lat.reunitarize()
+        lat.save_links()
+        ps0, pt0 = lat.plaquette()
+        runs = [("fp64_exact_arith", gfc.options(precision=gfc.PREC_FP64_EXACT, stop_rule=gfc.STOP_EVERY)),
+                ("fp64_full", gfc.options(precision=gfc.PREC_FP64_FULL, stop_rule=gfc.STOP_EVERY)),
+                ("fp64_fast", gfc.options(precision=gfc.PREC_FP64_FAST, stop_rule=gfc.STOP_EVERY)),
+                ("mixed", gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY, refine_reunit=10))]
+        ref = None
+        for name, o in runs:
+            lat.restore_links()
+            lat.fix(params, o)            # warm (launch shapes, graphs, allocations)
+            lat.restore_links()
+            rc, rep = lat.fix(params, o)
+            ps, pt = lat.plaquette()
+            d = dict(seconds=rep.seconds_total, sweeps=rc, final_e2=rep.final_residue, functional=rep.functional,
+                     plaq_drift=max(abs(ps - ps0), abs(pt - pt0)))
+            if name == "mixed":
+                d["sweeps_fp32"] = rep.sweeps_fp32
+            if ref is None:
+                ref = rep
+            else:
+                d["functional_vs_exact_arith"] = rep.functional - ref.functional
+            res[name] = d
+        res["mixed_speedup_vs_fp64_fast"] = res["fp64_fast"]["seconds"] / res["mixed"]["seconds"]
+        res["mixed_speedup_vs_fp64_full"] = res["fp64_full"]["seconds"] / res["mixed"]["seconds"]
+    raw.close()
     return res
 
 
@@ -457,7 +511,12 @@ def cpu_reference(a, steps, warmup, half_sweeps):
 
 def main():
     a = parse_args()
-    rk = Ranks()
+    # the reference arm is CPU work on rank 0 alone: no process group
+    rk = Ranks() if a.impl != "reference" else Ranks.__new__(Ranks)
+    if a.impl == "reference":
+        rk.world = int(os.environ.get("WORLD_SIZE", "1"))
+        rk.rank = int(os.environ.get("RANK", "0"))
+        rk.dist = None
     cfg = {"workload": f"{a.ns}^3x{a.nt} SU(3) Coulomb gauge fix to e2<={a.tol:g}, omega 1.95, hits 2",
            "lattice": [a.ns, a.nt], "seed": a.seed, "h_scale": a.scale, "tolerance": a.tol,
            "parallelism": f"replicas x{rk.world}" if rk.world > 1 else "1 GPU",
@@ -494,6 +553,8 @@ def main():
                 out["batch_mixed"] = run_batch(a, gfc, torch, gfc.PREC_MIXED)
             elif m == "batch64":
                 out["batch_fp64"] = run_batch(a, gfc, torch, gfc.PREC_FP64_FAST)
+            elif m == "precision":
+                out["precision_form"] = run_precision_form(a, gfc)
             elif m == "serve":
                 out["serve_mixed"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate)
             elif m == "serve64":
@@ -509,6 +570,8 @@ def main():
 
         import gfc
 
+        if not a.no_precision_form and not a.no_extras:
+            r["extras"]["precision_form"] = run_precision_form(a, gfc)
         if not a.no_batch:
             r["extras"]["batch_mixed"] = run_batch(a, gfc, torch, gfc.PREC_MIXED)
         if a.serve_requests > 0:

@@ -673,3 +673,36 @@ extern "C" int gfc_ctx_fix(gfc_ctx *c, const gfc_params *p, const gfc_options *o
     r->kernel_launches = (int)(c->launches - l0);
     return ret;
 }
+
+// gaugefixOverrelaxation(U, G, params) on host arrays in the reference layout
+// (src/gauge_fixing.c:713-826, declared include/gauge_fixing.h:67-69): U (4V
+// matrices, FP64, native endian) is fixed in place, G (V matrices) receives the
+// transformation.  A device context lives for the call.  Returns the reference's
+// values: half-sweeps, GFC_FIX_NOT_CONVERGED (-1; U and G are still written, as
+// the reference leaves them) or GFC_FIX_BAD_PARAMS (-2; nothing touched); below -2
+// a library error.
+extern "C" int gfc_gaugefix_overrelaxation(int ns, int nt, double *U, double *G, const gfc_params *p,
+                                           const gfc_options *opt, gfc_report *rep, int device) {
+    if (!U || !G || !p) return GFC_ERR_ARG;
+    if (!gfc_params_valid(p)) return GFC_FIX_BAD_PARAMS;
+    gfc_options od;
+    if (!opt) {
+        gfc_options_default(&od);
+        opt = &od;
+    }
+    gfc_ctx *c = nullptr;
+    int rc = gfc_ctx_create(ns, nt, device, opt->precision == GFC_PREC_MIXED ? GFC_CTX_MIXED : 0, &c);
+    if (rc) return rc;
+    rc = gfc_ctx_upload_links(c, U, 8, 0);
+    int fx = rc;
+    if (!rc) {
+        fx = gfc_ctx_fix(c, p, opt, rep);
+        if (fx >= 0 || fx == GFC_FIX_NOT_CONVERGED) {
+            rc = gfc_ctx_download_links(c, U, 8, 0);
+            if (!rc) rc = gfc_ctx_download_gt(c, G, 8, 0);
+            if (rc) fx = rc;
+        }
+    }
+    gfc_ctx_destroy(c);
+    return fx;
+}

@@ -121,6 +121,8 @@ def _load():
         "gfc_ctx_halfsweeps": (I, [P, I, I, ctypes.c_float, U, I]),
         "gfc_ctx_finalize_temporal": (I, [P]),
         "gfc_ctx_fix": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), ctypes.POINTER(Report)]),
+        "gfc_gaugefix_overrelaxation": (I, [I, I, P, P, ctypes.POINTER(Params), ctypes.POINTER(Options),
+                                            ctypes.POINTER(Report), I]),
         "gfc_e2_theta_device_noalloc": (I, [I, I, P, P, DP, DP]),
         "gfc_ctx_autotune": (I, [P, I, P]),
         "gfc_ctx_get_shapes": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]),
@@ -347,19 +349,22 @@ class Lattice:
 
 
 def gaugefix_overrelaxation(U, G, ns, nt, params=None, opts=None, device=0):
-    """Drop-in of gaugefixOverrelaxation(U, G, params) on host arrays.
+    """Drop-in of gaugefixOverrelaxation(U, G, params) on host arrays
+    (gfc_gaugefix_overrelaxation).
 
     U: float64 array of 4V*18 (reference layout), fixed in place; G: float64 array
     of V*18, overwritten with the gauge transformation.  Returns the reference's
     return value (sweeps, -1 or -2) and the run report.
     """
+    p = params if params is not None else default_params()
     o = opts if opts is not None else options()
-    with Lattice(ns, nt, device=device, mixed=(o.precision == PREC_MIXED)) as lat:
-        lat.upload_links(U, 8, False)
-        rc, rep = lat.fix(params, o)
-        if rc >= 0 or rc == FIX_NOT_CONVERGED:
-            lat.download_links(8, False, out=U)
-            lat.download_gt(8, False, out=G)
+    assert U.dtype == np.float64 and U.flags.c_contiguous and U.size == ns ** 3 * nt * 72
+    assert G.dtype == np.float64 and G.flags.c_contiguous and G.size == ns ** 3 * nt * 18
+    rep = Report()
+    rc = lib.gfc_gaugefix_overrelaxation(ns, nt, U.ctypes.data, G.ctypes.data, ctypes.byref(p), ctypes.byref(o),
+                                         ctypes.byref(rep), device)
+    if rc < FIX_BAD_PARAMS:
+        raise GFCError(f"gfc_gaugefix_overrelaxation failed ({rc}): {last_error()}")
     return rc, rep
 
 

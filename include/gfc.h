@@ -301,6 +301,14 @@ gfc_batch *gfc_server_batch(gfc_server *s);
  * -2 is a library error (gfc_last_error()).  opt may be NULL (reference behaviour). */
 int  gfc_ctx_fix(gfc_ctx *c, const gfc_params *p, const gfc_options *opt, gfc_report *rep);
 
+/* gaugefixOverrelaxation(U, G, params) (gauge_fixing.c:713-826, declared
+ * gauge_fixing.h:67-69) on host arrays in the reference layout: U (4V matrices of
+ * 9 complex doubles, native endian) is fixed in place and G (V matrices) receives
+ * the transformation; a device context lives for the call.  Same return values as
+ * gfc_ctx_fix; on -1 U and G are still written.  opt and rep may be NULL. */
+int  gfc_gaugefix_overrelaxation(int ns, int nt, double *U, double *G, const gfc_params *p,
+                                 const gfc_options *opt, gfc_report *rep, int device);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,33 @@ def test_exact_path_bit_for_bit(cases, tmp_path, name):
         # gauge-invariant value; ours stays equal to the value before (checked above).
 
 
+@pytest.mark.parametrize("name", ["l4x8", "cfg0_8x16", "l4x8_maxsweeps"])
+def test_one_shot_entry_point(cases, tmp_path, name):
+    """gfc_gaugefix_overrelaxation on host arrays, as the reference's main calls
+    gaugefixOverrelaxation(U, G, params) on a reunitarised U."""
+    c = cases[name]
+    ns, nt = c["ns"], c["nt"]
+    U = gfc.synth_config(ns, nt, c["seed"], c["scale"])
+    if c["in_bytes"] == 4:
+        pytest.skip("FP32 input goes through the file path")
+    orc.reunitarize(U)
+    G = np.empty(ns ** 3 * nt * 18)
+    rc, rep = gfc.gaugefix_overrelaxation(U, G, ns, nt, case_params(c, tmp_path),
+                                          gfc.options(precision=gfc.PREC_FP64_EXACT))
+    assert rc == c["sweeps"]
+    assert orc.sha(G) == c["gt_sha256"]
+    assert orc.sha(U.reshape(-1, 4, 18)[:, 1:4, :]) == c["u_spatial_sha256"]
+
+
+def test_one_shot_bad_params_touch_nothing():
+    U = gfc.synth_config(2, 4, 5, 0.5)
+    U0 = U.copy()
+    G = np.zeros(2 ** 3 * 4 * 18)
+    rc, _ = gfc.gaugefix_overrelaxation(U, G, 2, 4, gfc.default_params(omega_OR=2.5))
+    assert rc == gfc.FIX_BAD_PARAMS
+    assert np.array_equal(U, U0) and not G.any()
+
+
 def test_fp32_input_bit_for_bit(cases, tmp_path):
     c = cases["l4x8_f32in"]
     with gfc.Lattice(c["ns"], c["nt"]) as lat:
