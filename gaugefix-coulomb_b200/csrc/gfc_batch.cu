@@ -17,10 +17,10 @@
 // All parameters live in device memory, so one round is captured once as a CUDA
 // graph and replayed; the host only reads the state table between rounds.
 //
-// Inside a sweep kernel the last chunk of a timeslice to finish (ticket counter)
-// sums the chunk partials of the fused e2 in chunk order, adds the other parity's
-// contribution from the previous half-sweep (ring buffer) and decides the switch or
-// the retirement of that timeslice alone.
+// The sweep kernels write one pair of fused-e2 partials per chunk; after each
+// half-sweep k_bslice sums each timeslice's partials in a fixed order, adds the
+// other parity's contribution from the previous half-sweep (ring buffer) and
+// decides the switch or the retirement of that timeslice alone.
 //
 // Slots can be added, activated, finalised and removed between rounds, which is
 // what the serving loop does (continuous batching).
@@ -46,7 +46,6 @@ struct BSlot {          // device-visible descriptor of one resident lattice
     double2 *u64r, *g64r;  // FP64 two-row working copies
     float4 *u32, *g32;     // FP32 two-row working copies
     double *part;          // [nt][nbx][2] chunk partials of the fused e2
-    unsigned *tickets;     // [nt]
     int nbx;               // chunks per timeslice and parity = ceil(vs/2 / BCHUNK)
     int nfull;             // chunks per timeslice over both parities = ceil(vs / BCHUNK)
 };
@@ -56,6 +55,7 @@ struct BState {
     int max_nt, nslices;
     int *state;           // [nslices], gid = slot * max_nt + t
     int *sweeps;          // [nslices] half-sweeps applied to the timeslice
+    int *listed;          // [nslices] 1 if this round's sweep work lists hold the timeslice
     double *ring;         // [2][nslices][2]: (pre, post) e2 sums of the last two half-sweeps
     int2 *items32, *items64, *pend;
     int cap_items, cap_pend;
@@ -76,6 +76,7 @@ __global__ void __launch_bounds__(1024) k_compact(BState b) {
     int c[3] = {0, 0, 0}, act = 0;
     for (int gid = g0; gid < g1; gid++) {
         int st = b.state[gid];
+        b.listed[gid] = st == SS_FP32 || st == SS_FP64;
         if (st == SS_EMPTY || st == SS_DONE) continue;
         const BSlot &sl = b.slots[gid / b.max_nt];
         act++;
@@ -164,12 +165,14 @@ __device__ __forceinline__ void block_pair_sum(double &x, double &y, double (*sh
     __syncthreads();
 }
 
-template <class S, int MINB>
+// STG: the six links of a site are staged in shared memory by cp.async (dynamic
+// shared memory of 6 x NS x BCHUNK x 16 bytes), as in the single-lattice kernel
+template <class S, int MINB, bool STG>
 __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
+    extern __shared__ __align__(16) unsigned char bstage[];
     using T = typename S::T;
     constexpr bool F64 = sizeof(T) == 8;
     __shared__ double sh[2][BCHUNK / 32];
-    __shared__ int last;
     __shared__ int next[2];
     const int n = b.counts[F64 ? 1 : 0];
     const int k = b.counts[4];
@@ -202,46 +205,68 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
             const uint32_t vsh = l.vs >> 1;
             const uint32_t off = (uint32_t)chunk * BCHUNK + threadIdx.x;
             double pre = 0.0, post = 0.0;
-            if (off < vsh) fast_site<S>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, 1, pre, post);
+            if (off < vsh) {
+                if constexpr (STG)
+                    fast_site_staged<S, BCHUNK, false>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, 1,
+                                                       pre, post, (typename S::V *)bstage);
+                else
+                    fast_site<S>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, 1, pre, post);
+            }
             // chunk partials (deterministic order inside the block)
+            // the chunk's partials; k_bslice combines them after the half-sweep
             block_pair_sum(pre, post, sh);
             if (threadIdx.x == 0) {
                 double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
                 pp[0] = pre;
                 pp[1] = post;
-                __threadfence();
-                last = atomicAdd(&sl.tickets[t], 1u) == (unsigned)sl.nbx - 1;
-            }
-            __syncthreads();
-            if (last) {   // uniform: the CTA that completed the timeslice sums its partials
-                double s0 = 0.0, s1 = 0.0;
-                const double *pp = sl.part + (size_t)t * sl.nbx * 2;
-                for (int q = threadIdx.x; q < sl.nbx; q += BCHUNK) {
-                    s0 += __ldcg(pp + 2 * q);
-                    s1 += __ldcg(pp + 2 * q + 1);
-                }
-                block_pair_sum(s0, s1, sh);
-                if (threadIdx.x == 0) {
-                    sl.tickets[t] = 0;
-                    double *rprev = b.ring + ((size_t)((k + 1) & 1) * b.nslices + gid) * 2;
-                    double *rcur = b.ring + ((size_t)(k & 1) * b.nslices + gid) * 2;
-                    // e2 of the timeslice after k half-sweeps
-                    const double e2s = (s0 + __ldcg(rprev + 1)) / (double)l.vs;
-                    rcur[0] = s0;
-                    rcur[1] = s1;
-                    b.sweeps[gid] += 1;
-                    if (!(s0 == s0) || !(s1 == s1)) {
-                        atomicOr(b.status, GFC_STATUS_NAN);
-                        b.state[gid] = SS_DONE;
-                    } else if (!F64 && e2s <= b.switch_e2) {
-                        b.state[gid] = SS_PEND;
-                    } else if (F64 && e2s <= b.tol) {
-                        b.state[gid] = SS_DONE;
-                    }
-                }
             }
         }
         if (threadIdx.x == 0) next[(j + 1) & 1] = ahead;
+    }
+}
+
+// After both sweep kernels of a half-sweep: one warp per swept timeslice sums its
+// chunk partials in a fixed order (lane-strided, then a shuffle tree), records the
+// timeslice's e2 after k half-sweeps and retires it: FP32 -> pending switch at the
+// switch threshold, FP64 -> done at the tolerance, NaN -> done with the status bit.
+__global__ void k_bslice(BState b) {
+    const int lane = threadIdx.x & 31;
+    const int k = b.counts[4];
+    for (int gid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gid < b.nslices;
+         gid += (gridDim.x * blockDim.x) >> 5) {
+        const int st = b.state[gid];
+        // swept in this half-sweep: listed at the round's start and not retired since
+        // (a timeslice switched to FP64 at the start of the round has no items yet)
+        if (!b.listed[gid] || (st != SS_FP32 && st != SS_FP64)) continue;   // uniform in the warp
+        const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
+        const BSlot &sl = b.slots[slot];
+        const double *pp = sl.part + (size_t)t * sl.nbx * 2;
+        double s0 = 0.0, s1 = 0.0;
+        for (int q = lane; q < sl.nbx; q += 32) {
+            s0 += pp[2 * q];
+            s1 += pp[2 * q + 1];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s0 += __shfl_down_sync(0xffffffffu, s0, o);
+            s1 += __shfl_down_sync(0xffffffffu, s1, o);
+        }
+        if (lane == 0) {
+            double *rprev = b.ring + ((size_t)((k + 1) & 1) * b.nslices + gid) * 2;
+            double *rcur = b.ring + ((size_t)(k & 1) * b.nslices + gid) * 2;
+            const double e2s = (s0 + rprev[1]) / (double)sl.l.vs;   // e2 of the timeslice after k half-sweeps
+            rcur[0] = s0;
+            rcur[1] = s1;
+            b.sweeps[gid] += 1;
+            if (!(s0 == s0) || !(s1 == s1)) {
+                atomicOr(b.status, GFC_STATUS_NAN);
+                b.state[gid] = SS_DONE;
+            } else if (st == SS_FP32 && e2s <= b.switch_e2) {
+                b.state[gid] = SS_PEND;
+            } else if (st == SS_FP64 && e2s <= b.tol) {
+                b.state[gid] = SS_DONE;
+            }
+        }
     }
 }
 
@@ -395,7 +420,7 @@ struct gfc_batch {
     std::vector<void *> mem;        // per-slot allocation
     std::vector<int> used, ns, nt, activated;
     BSlot *dslots = nullptr;
-    int *state = nullptr, *sweeps = nullptr, *counts = nullptr;
+    int *state = nullptr, *sweeps = nullptr, *counts = nullptr, *listed = nullptr;
     double *ring = nullptr;
     int2 *items32 = nullptr, *items64 = nullptr, *pend = nullptr;
     int cap_items = 0, cap_pend = 0;
@@ -411,7 +436,7 @@ struct gfc_batch {
     int round_k = 8;
     BState captured{};
     int grid = 0, nsm = 0;
-    int minb32 = 4, minb64 = 3;
+    int minb32 = 4, minb64 = 3, stage64 = 1;
     // slot memory: a pool of its own that keeps freed memory mapped, so a slot
     // freed and another admitted costs no unmapping and remapping of device memory
     cudaMemPool_t pool = nullptr;
@@ -453,6 +478,8 @@ extern "C" int gfc_batch_create(int device, size_t max_sites, int max_slots, int
     BTRY(cudaMalloc(&b->state, sizeof(int) * b->nslices));
     BTRY(cudaMemset(b->state, 0, sizeof(int) * b->nslices));
     BTRY(cudaMalloc(&b->sweeps, sizeof(int) * b->nslices));
+    BTRY(cudaMalloc(&b->listed, sizeof(int) * b->nslices));
+    BTRY(cudaMemset(b->listed, 0, sizeof(int) * b->nslices));
     BTRY(cudaMemset(b->sweeps, 0, sizeof(int) * b->nslices));
     BTRY(cudaMalloc(&b->ring, sizeof(double) * 4 * b->nslices));
     BTRY(cudaMalloc(&b->items32, sizeof(int2) * b->cap_items));
@@ -502,6 +529,7 @@ extern "C" int gfc_batch_destroy(gfc_batch *b) {
     cudaFree(b->dslots);
     cudaFree(b->state);
     cudaFree(b->sweeps);
+    cudaFree(b->listed);
     cudaFree(b->ring);
     cudaFree(b->items32);
     cudaFree(b->items64);
@@ -526,7 +554,7 @@ extern "C" size_t gfc_batch_slot_bytes(int ns, int nt) {
     return al256(3 * 2 * vh * 9 * 16) + 2 * al256(2 * vh * 9 * 16)            // u, ut, g
            + al256(3 * 2 * vh * 6 * 16) + al256(2 * vh * 6 * 16)              // u64r, g64r
            + al256(3 * 2 * vh * 3 * 16) + al256(2 * vh * 3 * 16)              // u32, g32
-           + al256((size_t)nt * nbx * 2 * 8) + al256((size_t)nt * 4) + 4096;  // part, tickets
+           + al256((size_t)nt * nbx * 2 * 8) + 4096;  // chunk partials
 }
 
 extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
@@ -587,8 +615,6 @@ extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
     sl.nbx = (int)(((sl.l.vs >> 1) + BCHUNK - 1) / BCHUNK);
     sl.nfull = (int)((sl.l.vs + BCHUNK - 1) / BCHUNK);
     sl.part = (double *)take((size_t)nt * sl.nbx * 2 * 8);
-    sl.tickets = (unsigned *)take((size_t)nt * 4);
-    GFC_CHECK(cudaMemsetAsync(sl.tickets, 0, (size_t)nt * 4, b->s));
     GFC_CHECK(cudaMemcpyAsync(b->dslots + slot, &sl, sizeof sl, cudaMemcpyHostToDevice, b->s));
     GFC_CHECK(cudaStreamSynchronize(b->s));   // the host copy of sl goes out of scope
     b->hs[slot] = sl;
@@ -709,6 +735,7 @@ static BState make_state(gfc_batch *b, const gfc_params *p, const gfc_options *o
     s.nslices = b->nslices;
     s.state = b->state;
     s.sweeps = b->sweeps;
+    s.listed = b->listed;
     s.ring = b->ring;
     s.items32 = b->items32;
     s.items64 = b->items64;
@@ -727,13 +754,42 @@ static BState make_state(gfc_batch *b, const gfc_params *p, const gfc_options *o
     return s;
 }
 
+template <class S, int MINB, bool STG>
+static void launch_bsweep_k(int grid, cudaStream_t st, const BState &bs) {
+    constexpr size_t bytes = STG ? (size_t)6 * S::NS * BCHUNK * 16 : 0;
+    auto kern = k_bsweep<S, MINB, STG>;
+    if constexpr (STG) {
+        static unsigned long long done = 0;   // attribute set once per device
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 64 && !(done >> dev & 1ull)) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+            done |= 1ull << dev;
+        }
+    }
+    kern<<<grid, BCHUNK, bytes, st>>>(bs);
+}
+
+// minb: minimum resident CTAs per SM (1..4); stage: FP64 links staged in shared
+// memory (two-row FP64 only; 72 KiB per CTA, so at most 3 CTAs per SM)
 template <class S>
-static void launch_bsweep(int minb, int grid, cudaStream_t st, const BState &bs) {
+static void launch_bsweep(int minb, bool stage, int grid, cudaStream_t st, const BState &bs) {
+    if constexpr (sizeof(typename S::T) == 8) {
+        if (stage) {
+            switch (minb) {
+                case 1: return launch_bsweep_k<S, 1, true>(grid, st, bs);
+                case 2: return launch_bsweep_k<S, 2, true>(grid, st, bs);
+                default: return launch_bsweep_k<S, 3, true>(grid, st, bs);
+            }
+        }
+    }
     switch (minb) {
-        case 1: k_bsweep<S, 1><<<grid, BCHUNK, 0, st>>>(bs); break;
-        case 2: k_bsweep<S, 2><<<grid, BCHUNK, 0, st>>>(bs); break;
-        case 3: k_bsweep<S, 3><<<grid, BCHUNK, 0, st>>>(bs); break;
-        default: k_bsweep<S, 4><<<grid, BCHUNK, 0, st>>>(bs); break;
+        case 1: return launch_bsweep_k<S, 1, false>(grid, st, bs);
+        case 2: return launch_bsweep_k<S, 2, false>(grid, st, bs);
+        case 3: return launch_bsweep_k<S, 3, false>(grid, st, bs);
+        default: return launch_bsweep_k<S, 4, false>(grid, st, bs);
     }
 }
 
@@ -747,8 +803,10 @@ static void enqueue_round(gfc_batch *b, const BState &bs) {
     for (int k = 0; k < b->round_k; k++) {
         // one resident wave of persistent CTAs: a CTA that had to wait for a slot
         // would start its share of the items late and stretch the tail
-        launch_bsweep<S32>(b->minb32, b->nsm * b->minb32, st, bs);
-        launch_bsweep<S64R>(b->minb64, b->nsm * b->minb64, st, bs);
+        const int m64 = b->stage64 ? std::min(b->minb64, 3) : b->minb64;
+        launch_bsweep<S32>(b->minb32, false, b->nsm * b->minb32, st, bs);
+        launch_bsweep<S64R>(m64, b->stage64 != 0, b->nsm * m64, st, bs);
+        k_bslice<<<(b->nslices + 7) / 8, 256, 0, st>>>(bs);
         k_btick<<<1, 32, 0, st>>>(bs);
         k_breunit<S32><<<b->grid, BCHUNK, 0, st>>>(bs, bs.reunit32);
         k_breunit<S64R><<<b->grid, BCHUNK, 0, st>>>(bs, bs.reunit64);
@@ -788,7 +846,7 @@ extern "C" int gfc_batch_round(gfc_batch *b, const gfc_params *p, const gfc_opti
     int rc = ensure_graph(b, p, o);
     if (rc) return rc;
     GFC_CHECK(cudaGraphLaunch(b->exec, b->s));
-    b->launches += 4 + 5 * b->round_k;
+    b->launches += 4 + 6 * b->round_k;
     b->rounds++;
     GFC_CHECK(cudaMemcpyAsync(b->hcounts, b->counts, sizeof(int) * 8, cudaMemcpyDeviceToHost, b->s));
     GFC_CHECK(cudaMemcpyAsync(b->hstate, b->state, sizeof(int) * b->nslices, cudaMemcpyDeviceToHost, b->s));
@@ -990,6 +1048,125 @@ extern "C" int gfc_batch_set_shape(gfc_batch *b, int minb32, int minb64, int rou
         cudaGraphDestroy(b->graph);
         b->graph = nullptr;
     }
+    return GFC_OK;
+}
+
+// FP64 links staged in shared memory by the batch sweep (1) or not (0)
+extern "C" int gfc_batch_set_staging(gfc_batch *b, int stage64) {
+    if (!b) return GFC_ERR_ARG;
+    b->stage64 = stage64 != 0;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return GFC_OK;
+}
+
+extern "C" int gfc_batch_get_shape(const gfc_batch *b, int *minb32, int *minb64, int *stage64, int *round_sweeps) {
+    if (!b) return GFC_ERR_ARG;
+    if (minb32) *minb32 = b->minb32;
+    if (minb64) *minb64 = b->stage64 ? std::min(b->minb64, 3) : b->minb64;
+    if (stage64) *stage64 = b->stage64;
+    if (round_sweeps) *round_sweeps = b->round_k;
+    return GFC_OK;
+}
+
+// Times the batch's launch shapes on a scratch lattice of the given size (seeded
+// synthetic links) and keeps the fastest: resident CTAs per SM of the FP32 sweep,
+// resident CTAs and shared-memory staging of the FP64 sweep, then half-sweeps per
+// captured round.  The batch must have no activated slot; the scratch slot is
+// removed again.  times (may be NULL, GFC_BATCH_TUNE_SLOTS entries) receives seconds
+// per half-sweep: [0..2] FP32 minb 2,3,4; [3..7] FP64 (minb, staged) (2,0) (3,0)
+// (4,0) (2,1) (3,1); [8..10] rounds of 4, 8, 16 half-sweeps.
+extern "C" int gfc_batch_autotune(gfc_batch *b, int ns, int nt, double *times) {
+    if (!b) return GFC_ERR_ARG;
+    for (int k = 0; k < b->max_slots; k++)
+        if (b->used[k] && b->activated[k]) {
+            set_error("autotune needs a batch without activated slots");
+            return GFC_ERR_STATE;
+        }
+    double t[GFC_BATCH_TUNE_SLOTS] = {0};
+    int slot = -1;
+    int rc = gfc_batch_add(b, ns, nt, &slot);
+    if (rc) return rc;
+    gfc_params pt;
+    gfc_params_default(&pt);
+    pt.tolerance = 1e-300;   // nothing retires while timing
+    gfc_options ot;
+    gfc_options_default(&ot);
+    ot.switch_e2 = 1e-300;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const int save32 = b->minb32, save64 = b->minb64, saves = b->stage64, savek = b->round_k;
+    auto time_rounds = [&](int prec, double &out) -> int {
+        ot.precision = prec;
+        int active = 0, r = gfc_batch_round(b, &pt, &ot, &active);   // warm: capture + first round
+        if (r) return r;
+        GFC_CHECK(cudaEventRecord(e0, b->s));
+        for (int q = 0; q < 3; q++)
+            if ((r = gfc_batch_round(b, &pt, &ot, &active))) return r;
+        GFC_CHECK(cudaEventRecord(e1, b->s));
+        GFC_CHECK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        GFC_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        out = ms * 1e-3 / (3.0 * b->round_k);
+        return GFC_OK;
+    };
+    int best32 = save32, best64 = save64, bests = saves, bestk = savek;
+    auto ce = [](cudaError_t e) { return e == cudaSuccess ? GFC_OK : cuda_fail(e, "cudaEventCreate"); };
+    do {
+        if ((rc = ce(cudaEventCreate(&e0)))) break;
+        if ((rc = ce(cudaEventCreate(&e1)))) break;
+        if ((rc = gfc_batch_synth(b, slot, 1, 0.5))) break;
+        // FP32 sweep
+        if ((rc = gfc_batch_activate(b, slot, GFC_PREC_MIXED))) break;
+        double best = 1e30;
+        const int m32[3] = {2, 3, 4};
+        for (int q = 0; q < 3 && !rc; q++) {
+            gfc_batch_set_shape(b, m32[q], save64, 4);
+            rc = time_rounds(GFC_PREC_MIXED, t[q]);
+            if (!rc && t[q] < best) best = t[q], best32 = m32[q];
+        }
+        if (rc) break;
+        // FP64 sweep
+        if ((rc = gfc_batch_activate(b, slot, GFC_PREC_FP64_FAST))) break;
+        best = 1e30;
+        const int m64[5] = {2, 3, 4, 2, 3}, st64[5] = {0, 0, 0, 1, 1};
+        for (int q = 0; q < 5 && !rc; q++) {
+            gfc_batch_set_shape(b, best32, m64[q], 4);
+            gfc_batch_set_staging(b, st64[q]);
+            rc = time_rounds(GFC_PREC_FP64_FAST, t[3 + q]);
+            if (!rc && t[3 + q] < best) best = t[3 + q], best64 = m64[q], bests = st64[q];
+        }
+        if (rc) break;
+        // half-sweeps per round (FP64 work; the per-round compaction is amortised)
+        best = 1e30;
+        const int ks[3] = {4, 8, 16};
+        gfc_batch_set_staging(b, bests);
+        for (int q = 0; q < 3 && !rc; q++) {
+            gfc_batch_set_shape(b, best32, best64, ks[q]);
+            rc = time_rounds(GFC_PREC_FP64_FAST, t[8 + q]);
+            if (!rc && t[8 + q] < best * 0.98) best = t[8 + q], bestk = ks[q];
+        }
+    } while (0);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    k_set_state<<<(nt + 127) / 128, 128, 0, b->s>>>(b->state, slot * b->max_nt, nt, SS_EMPTY);
+    b->activated[slot] = 0;
+    int rc2 = gfc_batch_remove(b, slot);
+    if (!rc) rc = rc2;
+    if (rc) {
+        gfc_batch_set_shape(b, save32, save64, savek);
+        gfc_batch_set_staging(b, saves);
+        return rc;
+    }
+    gfc_batch_set_shape(b, best32, best64, bestk);
+    gfc_batch_set_staging(b, bests);
+    if (times)
+        for (int q = 0; q < GFC_BATCH_TUNE_SLOTS; q++) times[q] = t[q];
     return GFC_OK;
 }
 

@@ -68,8 +68,18 @@ struct SweepArgs {
 struct Shape {
     int block, minb;
 };
-constexpr Shape kShapes[] = {{128, 2}, {128, 3}, {128, 4}, {64, 4}, {64, 6}, {256, 1}, {256, 2}};
+constexpr Shape kShapes[] = {{128, 2}, {128, 3}, {128, 4}, {64, 4}, {64, 6}, {256, 1}, {256, 2}, {128, 5}, {128, 6}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+// Shapes of the shared-memory staged kernel (two-row storage only): the six links
+// and, with sg, G are copied to shared memory by cp.async before the update
+// (6 or 7 x 96 B per thread in FP64, 48 B in FP32), which also bounds residency.
+struct SShape {
+    int block, minb, sg;
+};
+constexpr SShape kStaged[] = {{128, 2, 1}, {64, 5, 1}, {128, 3, 0}, {256, 1, 1}, {128, 4, 1}, {128, 5, 1}};
+constexpr int kNumStaged = sizeof(kStaged) / sizeof(kStaged[0]);
+constexpr int kNumAll = kNumShapes + kNumStaged;   // shape indices: plain, then staged
+static_assert(3 + 2 * kNumAll + 8 == GFC_TUNE_SLOTS, "autotune time slots");
 constexpr int MIN_BLOCK = 64;   // smallest block: sizes the per-block partial buffers
 
 // deterministic sum of NQ values over the block; result in thread 0
@@ -177,6 +187,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_fast(typename S::V *__res
     const bool active = off < vsh;
     double pre = 0.0, post = 0.0;
     if (active) fast_site<S>(u, g, l, a.par, (a.t0 + blockIdx.y) * vsh + off, (T)a.omega, a.hits, a.track, pre, post);
+    if (a.track) fused_reduce<BLOCK>(a, pre, post);
+}
+
+template <class S, int BLOCK, int MINB, bool SG>
+__global__ void __launch_bounds__(BLOCK, MINB) k_sweep_staged(typename S::V *__restrict__ u,
+                                                              typename S::V *__restrict__ g, SweepArgs a) {
+    extern __shared__ __align__(16) unsigned char staged_smem[];
+    using T = typename S::T;
+    if (a.stop && *(volatile unsigned *)a.stop) return;
+    const Lat &l = a.l;
+    const uint32_t vsh = l.vs >> 1;
+    const uint32_t off = blockIdx.x * BLOCK + threadIdx.x;
+    double pre = 0.0, post = 0.0;
+    if (off < vsh)
+        fast_site_staged<S, BLOCK, SG>(u, g, l, a.par, (a.t0 + blockIdx.y) * vsh + off, (T)a.omega, a.hits, a.track,
+                                       pre, post, (typename S::V *)staged_smem);
     if (a.track) fused_reduce<BLOCK>(a, pre, post);
 }
 
@@ -331,8 +357,45 @@ static void launch_shape(dim3 grid, cudaStream_t st, typename S::V *u, typename 
 }
 
 template <class S>
+static constexpr size_t staged_bytes(int block, int sg) {
+    return (size_t)(6 + sg) * S::NS * block * 16;
+}
+
+template <class S, int K>
+static void launch_staged(dim3 grid, cudaStream_t st, typename S::V *u, typename S::V *g, const SweepArgs &a) {
+    constexpr SShape sh = kStaged[K];
+    constexpr size_t bytes = staged_bytes<S>(sh.block, sh.sg);
+    static_assert(bytes <= 227 * 1024, "staged tile exceeds shared memory");
+    auto kern = k_sweep_staged<S, sh.block, sh.minb, (bool)sh.sg>;
+    // the attribute is set once per device (a CUDA function attribute is per context)
+    static unsigned long long done = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !(done >> dev & 1ull)) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+        done |= 1ull << dev;
+    }
+    grid.x = ((a.l.vs >> 1) + sh.block - 1) / sh.block;
+    kern<<<grid, sh.block, bytes, st>>>(u, g, a);
+}
+
+template <class S>
 static void dispatch_fast(int v, dim3 grid, cudaStream_t st, typename S::V *u, typename S::V *g,
                           const SweepArgs &a) {
+    if constexpr (S::ROWS01_ONLY) {
+        switch (v - kNumShapes) {
+            case 0: return launch_staged<S, 0>(grid, st, u, g, a);
+            case 1: return launch_staged<S, 1>(grid, st, u, g, a);
+            case 2: return launch_staged<S, 2>(grid, st, u, g, a);
+            case 3: return launch_staged<S, 3>(grid, st, u, g, a);
+            case 4: return launch_staged<S, 4>(grid, st, u, g, a);
+            case 5: return launch_staged<S, 5>(grid, st, u, g, a);
+            default: break;
+        }
+    } else if (v >= kNumShapes) {
+        v = 1;   // full 3x3 storage has no staged form
+    }
     switch (v) {
         case 0: launch_shape<S, 0>(grid, st, u, g, a); break;
         case 1: launch_shape<S, 1>(grid, st, u, g, a); break;
@@ -340,7 +403,9 @@ static void dispatch_fast(int v, dim3 grid, cudaStream_t st, typename S::V *u, t
         case 3: launch_shape<S, 3>(grid, st, u, g, a); break;
         case 4: launch_shape<S, 4>(grid, st, u, g, a); break;
         case 5: launch_shape<S, 5>(grid, st, u, g, a); break;
-        default: launch_shape<S, 6>(grid, st, u, g, a); break;
+        case 6: launch_shape<S, 6>(grid, st, u, g, a); break;
+        case 7: launch_shape<S, 7>(grid, st, u, g, a); break;
+        default: launch_shape<S, 8>(grid, st, u, g, a); break;
     }
 }
 
@@ -661,7 +726,8 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
 // and keeps the fastest per kernel.  The links are saved first and restored after
 // (the timed half-sweeps change them), and G is reset to the identity.
 // times (optional, length >= GFC_TUNE_SLOTS) receives seconds per half-sweep:
-//   [0..2] exact shapes, [3..9] FP64 fast shapes, [10..16] FP32 shapes (0: not timed).
+//   [0..2] exact shapes, [3..17] FP64 fast shapes (9 plain, then 6 staged), [18..32]
+//   FP32 shapes, [33..36] FP64 slice blocking, [37..40] FP32 slice blocking (0: not timed).
 using namespace gfc;
 
 extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
@@ -727,7 +793,7 @@ extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
         if ((rc = ensure_2row(c))) return rc;
         pack_2row(c);
         double best = 1e30;
-        for (int v = 0; v < kNumShapes; v++) {
+        for (int v = 0; v < kNumAll; v++) {
             double t = timed(
                 [&](int k) { dispatch_fast<S64R>(v, dim3(0, l.nt), c->s, c->u64r, c->g64r, args_for(k)); });
             times[3 + v] = t;
@@ -742,11 +808,11 @@ extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
         k_to_f32<<<gu, 256, 0, c->s>>>(c->u, (float4 *)c->u32, l.vh, 3 * l.npar);
         k_identity32<<<gg, 256, 0, c->s>>>((float4 *)c->g32, l.vh, l.npar);
         double best = 1e30;
-        for (int v = 0; v < kNumShapes; v++) {
+        for (int v = 0; v < kNumAll; v++) {
             double t = timed([&](int k) {
                 dispatch_fast<S32>(v, dim3(0, l.nt), c->s, (float4 *)c->u32, (float4 *)c->g32, args_for(k));
             });
-            times[10 + v] = t;
+            times[3 + kNumAll + v] = t;
             if (t < best) {
                 best = t;
                 c->shape_fast32 = v;
@@ -791,17 +857,18 @@ extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
     };
     if (which & 2) {
         double base = 1e30;
-        for (int v = 0; v < kNumShapes; v++)
+        for (int v = 0; v < kNumAll; v++)
             if (times[3 + v] > 0 && times[3 + v] < base) base = times[3 + v];
-        rc = tune_blocking(S64R{}, c->u64r, c->g64r, 96, c->blk64_slices, c->blk64_sweeps, base, times + 17);
+        rc = tune_blocking(S64R{}, c->u64r, c->g64r, 96, c->blk64_slices, c->blk64_sweeps, base,
+                           times + 3 + 2 * kNumAll);
         if (rc) return rc;
     }
     if ((which & 4) && c->u32 && c->g32) {
         double base = 1e30;
-        for (int v = 0; v < kNumShapes; v++)
-            if (times[10 + v] > 0 && times[10 + v] < base) base = times[10 + v];
+        for (int v = 0; v < kNumAll; v++)
+            if (times[3 + kNumAll + v] > 0 && times[3 + kNumAll + v] < base) base = times[3 + kNumAll + v];
         rc = tune_blocking(S32{}, (float4 *)c->u32, (float4 *)c->g32, 48, c->blk32_slices, c->blk32_sweeps, base,
-                           times + 21);
+                           times + 7 + 2 * kNumAll);
         if (rc) return rc;
     }
     GFC_CHECK(cudaGetLastError());
@@ -847,7 +914,7 @@ extern "C" int gfc_ctx_get_shapes(const gfc_ctx *c, int *exact, int *fast64, int
 
 extern "C" int gfc_ctx_set_shapes(gfc_ctx *c, int exact, int fast64, int fast32) {
     if (!c) return GFC_ERR_ARG;
-    if (exact >= exact_num_shapes() || fast64 >= kNumShapes || fast32 >= kNumShapes) return GFC_ERR_ARG;
+    if (exact >= exact_num_shapes() || fast64 >= kNumAll || fast32 >= kNumAll) return GFC_ERR_ARG;
     if (exact >= 0) c->shape_exact = exact;
     if (fast64 >= 0) c->shape_fast64 = fast64;
     if (fast32 >= 0) c->shape_fast32 = fast32;

@@ -469,4 +469,171 @@ __device__ __forceinline__ void fast_site(typename S::V *__restrict__ u, typenam
     }
 }
 
+// ------------------------------------------------- shared-memory staging --
+// 16-byte asynchronous copy global -> shared (no registers held while in flight);
+// both addresses 16-byte aligned.  wait_all makes the thread's own copies visible
+// to that thread.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// up . f (forward link) or r . up^dagger (backward link) from a staged copy `src`
+// (stride sst) to global `dst` (stride st); rows 0 and 1 are stored, row 2 only
+// enters e2.
+template <class S, bool FWD>
+__device__ __forceinline__ void apply_staged(const typename S::V *src, int sst, typename S::V *__restrict__ dst,
+                                             size_t st, const Mt<typename S::T> &up, int track, double (&cc)[8]) {
+    using T = typename S::T;
+    using C = typename CT<T>::t;
+    const double sg = FWD ? 1.0 : -1.0;
+    if constexpr (S::ROWWISE) {
+        // one output row at a time; operands are read back from shared memory as
+        // needed rather than held (row 2 of the link is rebuilt from rows 0 and 1)
+        C r2[3];
+        if (FWD || track) {
+            C a[3] = {src[0], src[sst], src[2 * sst]};
+            C b[3] = {src[3 * sst], src[4 * sst], src[5 * sst]};
+            fcross_conj(a, b, r2);
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (r == 2 && !track) break;
+            C o[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C v;
+                if (FWD) {
+                    v = fmul(up.e[EL(r, 0)], (C)src[j * sst]);
+                    v = fadd(v, fmul(up.e[EL(r, 1)], (C)src[(3 + j) * sst]));
+                    v = fadd(v, fmul(up.e[EL(r, 2)], r2[j]));
+                } else {
+                    const C m0 = r < 2 ? (C)src[(3 * r) * sst] : r2[0];
+                    const C m1 = r < 2 ? (C)src[(3 * r + 1) * sst] : r2[1];
+                    const C m2 = r < 2 ? (C)src[(3 * r + 2) * sst] : r2[2];
+                    v = fmul_conj(m0, up.e[EL(j, 0)]);
+                    v = fadd(v, fmul_conj(m1, up.e[EL(j, 1)]));
+                    v = fadd(v, fmul_conj(m2, up.e[EL(j, 2)]));
+                }
+                o[j] = v;
+                if (r < 2) dst[(size_t)(3 * r + j) * st] = v;
+            }
+            if (track) {
+                if (r == 0) acc_row<0>(cc, o[0], o[1], o[2], sg);
+                if (r == 1) acc_row<1>(cc, o[0], o[1], o[2], sg);
+                if (r == 2) acc_row<2>(cc, o[0], o[1], o[2], sg);
+            }
+        }
+    } else {
+        Mt<T> m, o;
+        S::load(src, sst, m);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (r == 2 && !track) break;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C v;
+                if (FWD) {
+                    v = fmul(up.e[EL(r, 0)], m.e[EL(0, j)]);
+                    v = fadd(v, fmul(up.e[EL(r, 1)], m.e[EL(1, j)]));
+                    v = fadd(v, fmul(up.e[EL(r, 2)], m.e[EL(2, j)]));
+                } else {
+                    v = fmul_conj(m.e[EL(r, 0)], up.e[EL(j, 0)]);
+                    v = fadd(v, fmul_conj(m.e[EL(r, 1)], up.e[EL(j, 1)]));
+                    v = fadd(v, fmul_conj(m.e[EL(r, 2)], up.e[EL(j, 2)]));
+                }
+                o.e[EL(r, j)] = v;
+            }
+        }
+        S::store(dst, st, o);   // rows 0 and 1
+        if (track) {
+            acc_mat_row<0>(cc, o, sg);
+            acc_mat_row<1>(cc, o, sg);
+            acc_mat_row<2>(cc, o, sg);
+        }
+    }
+}
+
+// fast_site with the six links (and, with SG, G) first copied into shared memory
+// by cp.async: every byte the site needs is requested at once, without registers
+// held for it, and the link update reads its operands back from shared memory
+// instead of from L2.  Staged layout per CTA: entry e of matrix m of thread x at
+// sm[(m * NS + e) * BLOCK + x] (m = 2d forward, 2d+1 backward link of direction d,
+// m = 6 G).  Two-row storage only.
+template <class S, int BLOCK, bool SG>
+__device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, typename S::V *__restrict__ g,
+                                                 const Lat &l, int par, uint32_t i, typename S::T omega,
+                                                 unsigned hits, int track, double &pre, double &post,
+                                                 typename S::V *sm) {
+    using T = typename S::T;
+    using C = typename CT<T>::t;
+    using V = typename S::V;
+    static_assert(S::ROWS01_ONLY, "staging is for two-row storage");
+    const int op = par ^ 1;
+    Coord c = coord_cb(l, par, i);
+    uint32_t ib[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) ib[d] = back_L(l, c, d) >> 1;
+    V *my = sm + threadIdx.x;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const V *f = u + su_idx<S>(l, d, par, i);
+        const V *r = u + su_idx<S>(l, d, op, ib[d]);
+#pragma unroll
+        for (int e = 0; e < S::NS; e++) {
+            cp_async16(my + ((2 * d) * S::NS + e) * BLOCK, f + (size_t)e * l.vh);
+            cp_async16(my + ((2 * d + 1) * S::NS + e) * BLOCK, r + (size_t)e * l.vh);
+        }
+    }
+    if (SG) {
+        const V *gp = g + sg_idx<S>(l, par, i);
+#pragma unroll
+        for (int e = 0; e < S::NS; e++) cp_async16(my + (6 * S::NS + e) * BLOCK, gp + (size_t)e * l.vh);
+    }
+    cp_async_wait_all();
+
+    Mt<T> w;
+#pragma unroll
+    for (int k = 0; k < 9; k++) w.e[k] = mkc<C>(T(0), T(0));
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        Mt<T> f, r;
+        S::load(my + (2 * d) * S::NS * BLOCK, BLOCK, f);
+        S::load(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, r);
+#pragma unroll
+        for (int x = 0; x < 3; x++)
+#pragma unroll
+            for (int y = 0; y < 3; y++) w.e[EL(x, y)] = fadd(w.e[EL(x, y)], fadd(f.e[EL(x, y)], fconj(r.e[EL(y, x)])));
+    }
+    if (track) pre = e2_from_w(w);
+
+    Mt<T> up;
+    fupdate(w, omega, hits, up);
+    // the links are read again from shared memory below: keep the compiler from
+    // holding the values loaded for w(x) in registers across the update instead
+    asm volatile("" ::: "memory");
+    {
+        Mt<T> m, o;
+        if (SG)
+            S::load(my + 6 * S::NS * BLOCK, BLOCK, m);
+        else
+            S::load(g + sg_idx<S>(l, par, i), l.vh, m);
+        fprod_left<S>(up, m, o);
+        S::store(g + sg_idx<S>(l, par, i), l.vh, o);
+    }
+    double cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        apply_staged<S, true>(my + (2 * d) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, par, i), l.vh, up, track, cc);
+        apply_staged<S, false>(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, op, ib[d]), l.vh, up,
+                               track, cc);
+    }
+    if (track) {
+        cc[7] *= 0.57735026918962576451;
+#pragma unroll
+        for (int k = 0; k < 8; k++) post += cc[k] * cc[k];
+    }
+}
+
 }  // namespace gfc

@@ -286,10 +286,10 @@ class Lattice:
     def autotune(self, which=0):
         """Time every compiled launch shape on this lattice; keep the fastest.
         Returns seconds per half-sweep: {"exact": [...], "fast64": [...], "fast32": [...]}."""
-        t = np.zeros(25)
+        t = np.zeros(41)
         _check(lib.gfc_ctx_autotune(self.h, which, t.ctypes.data), "autotune")
-        return {"exact": t[0:3].tolist(), "fast64": t[3:10].tolist(), "fast32": t[10:17].tolist(),
-                "fast64_blocked": t[17:21].tolist(), "fast32_blocked": t[21:25].tolist()}
+        return {"exact": t[0:3].tolist(), "fast64": t[3:18].tolist(), "fast32": t[18:33].tolist(),
+                "fast64_blocked": t[33:37].tolist(), "fast32_blocked": t[37:41].tolist()}
 
     def set_blocking(self, precision_bits, slices, sweeps):
         _check(lib.gfc_ctx_set_blocking(self.h, precision_bits, slices, sweeps), "set_blocking")
@@ -393,6 +393,9 @@ def _bind_batch():
         "gfc_batch_kernel_launches": (ctypes.c_longlong, [P]),
         "gfc_batch_stream": (P, [P]),
         "gfc_batch_set_shape": (I, [P, I, I, I]),
+        "gfc_batch_set_staging": (I, [P, I]),
+        "gfc_batch_get_shape": (I, [P] + [IP] * 4),
+        "gfc_batch_autotune": (I, [P, I, I, ctypes.POINTER(D)]),
         "gfc_batch_fix_all": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), RP]),
     }
     for name, (res, args) in sig.items():
@@ -500,6 +503,21 @@ class Batch:
 
     def set_shape(self, minb32=4, minb64=3, round_sweeps=8):
         _check(lib.gfc_batch_set_shape(self.h, minb32, minb64, round_sweeps), "set_shape")
+
+    def set_staging(self, stage64):
+        _check(lib.gfc_batch_set_staging(self.h, int(stage64)), "set_staging")
+
+    def shape(self):
+        v = [ctypes.c_int() for _ in range(4)]
+        _check(lib.gfc_batch_get_shape(self.h, *[ctypes.byref(x) for x in v]), "get_shape")
+        return dict(minb32=v[0].value, minb64=v[1].value, stage64=v[2].value, round_sweeps=v[3].value)
+
+    def autotune(self, ns, nt):
+        """Time the launch shapes on a scratch ns^3 x nt lattice; keep the fastest."""
+        t = (ctypes.c_double * 11)()
+        _check(lib.gfc_batch_autotune(self.h, ns, nt, t), "gfc_batch_autotune")
+        return {"fp32_minb_2_3_4": list(t[0:3]), "fp64_minb_staged_20_30_40_21_31": list(t[3:8]),
+                "round_4_8_16": list(t[8:11])}
 
     @property
     def kernel_launches(self):
@@ -632,6 +650,13 @@ class Server:
 
     def release(self, rid):
         _check(lib.gfc_server_fetch(self.h, rid, None, 8, 1), "gfc_server_fetch")
+
+    def autotune(self, ns, nt):
+        """Launch shapes of the server's batch, timed on a scratch ns^3 x nt lattice
+        (before requests are admitted)."""
+        t = (ctypes.c_double * 11)()
+        _check(lib.gfc_batch_autotune(lib.gfc_server_batch(self.h), ns, nt, t), "gfc_batch_autotune")
+        return list(t)
 
     def batch_stream(self):
         return lib.gfc_batch_stream(lib.gfc_server_batch(self.h))

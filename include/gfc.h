@@ -189,12 +189,13 @@ int  gfc_ctx_finalize_temporal(gfc_ctx *c);
  * which: bit 0 exact FP64, bit 1 fast FP64, bit 2 FP32 (0 = all).  The links are
  * saved and restored around the timing (a device copy of all links is kept) and G
  * is reset to the identity.  times (may be NULL) receives seconds per half-sweep:
- * [0..2] exact shapes, [3..9] fast FP64 shapes, [10..16] FP32 shapes, [17..20] fast
- * FP64 slice-blocked candidates, [21..24] FP32 slice-blocked candidates.  Slice
+ * [0..2] exact shapes, [3..17] fast FP64 shapes (9 plain, then 6 with the links
+ * staged in shared memory by cp.async), [18..32] FP32 shapes (same order), [33..36]
+ * fast FP64 slice-blocked candidates, [37..40] FP32 slice-blocked candidates.  Slice
  * blocking runs a group of timeslices for several half-sweeps while its links stay in
  * L2 (timeslices share no link during the sweeps); it is kept only where it measured
  * faster. */
-#define GFC_TUNE_SLOTS 25
+#define GFC_TUNE_SLOTS 41
 int  gfc_ctx_autotune(gfc_ctx *c, int which, double *times);
 int  gfc_ctx_get_shapes(const gfc_ctx *c, int *exact, int *fast64, int *fast32);
 /* -1 keeps the current choice */
@@ -258,6 +259,16 @@ long long gfc_batch_kernel_launches(const gfc_batch *b);
 void  *gfc_batch_stream(gfc_batch *b);
 /* minimum resident CTAs per SM of the FP32 / FP64 sweep kernels (1..4) and half-sweeps per round */
 int    gfc_batch_set_shape(gfc_batch *b, int minb32, int minb64, int round_sweeps);
+/* FP64 batch sweep with the links staged in shared memory (1, default) or not (0) */
+int    gfc_batch_set_staging(gfc_batch *b, int stage64);
+int    gfc_batch_get_shape(const gfc_batch *b, int *minb32, int *minb64, int *stage64, int *round_sweeps);
+/* Time the launch shapes on a scratch lattice of size ns^3 x nt and keep the fastest
+ * (FP32 resident CTAs per SM, FP64 resident CTAs and staging, half-sweeps per round).
+ * Needs a batch without activated slots.  times (may be NULL): seconds per half-sweep,
+ * [0..2] FP32 minb 2,3,4; [3..7] FP64 (minb, staged) (2,0) (3,0) (4,0) (2,1) (3,1);
+ * [8..10] rounds of 4, 8, 16 half-sweeps. */
+#define GFC_BATCH_TUNE_SLOTS 11
+int    gfc_batch_autotune(gfc_batch *b, int ns, int nt, double *times);
 /* rounds until every activated slot retired (or max_sweeps), then finalise them;
  * reports indexed by slot; returns the number of rounds */
 int    gfc_batch_fix_all(gfc_batch *b, const gfc_params *p, const gfc_options *o, gfc_report *reports);

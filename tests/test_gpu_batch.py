@@ -125,3 +125,38 @@ def test_batch_admission_limits():
             b.add(6, 8)                  # 1728 more: over max_sites
         b.remove(s)
         b.add(6, 8)
+
+
+def test_batch_autotune_then_fix():
+    with gfc.Batch(max_sites=10 ** 6, max_slots=4, max_nt=16) as b:
+        times = b.autotune(8, 12)
+        assert all(t > 0 for v in times.values() for t in v)
+        shape = b.shape()
+        assert 2 <= shape["minb32"] <= 4 and shape["round_sweeps"] in (4, 8, 16)
+        with pytest.raises(gfc.GFCError):
+            s = b.add(6, 8)
+            b.upload(s, gfc.synth_config(6, 8, 5, 0.5), 8, False)
+            b.activate(s, gfc.PREC_MIXED)
+            b.autotune(8, 12)          # refused while a slot is being fixed
+        rounds, reps = b.fix_all(params(), gfc.options(precision=gfc.PREC_MIXED))
+        assert reps[s].status > 0 and reps[s].e2 <= 1.5 * TOL
+
+
+@pytest.mark.parametrize("stage", [0, 1])
+def test_staging_gives_a_valid_fix(stage):
+    ns, nt = 6, 8
+    U = gfc.synth_config(ns, nt, 95, 0.6)
+    with gfc.Batch(max_sites=10 ** 5, max_slots=2, max_nt=8) as b:
+        b.set_staging(stage)
+        s = b.add(ns, nt)
+        b.upload(s, U, 8, False)
+        orc.reunitarize(U)
+        b.activate(s, gfc.PREC_FP64_FAST)
+        rounds, reps = b.fix_all(params(), gfc.options(precision=gfc.PREC_FP64_FAST))
+        assert reps[s].e2 <= 1.5 * TOL
+        G = b.download_gt(s)
+        Uf = b.download_links(s)
+    assert su3_error(G) < 1e-13
+    U1 = U.copy()
+    orc.apply_gt(U1, G, ns, nt)
+    np.testing.assert_allclose(U1, Uf, atol=1e-12)

@@ -86,31 +86,41 @@ def test_fast_tracks_exact_per_sweep():
     assert out[gfc.PREC_FP64_FAST][1] == pytest.approx(out[gfc.PREC_FP64_EXACT][1], rel=1e-12)
 
 
-def test_every_launch_shape_gives_identical_results():
-    """The autotuner may pick any compiled shape: all of them compute the same bits."""
+N_PLAIN = 9   # plain shapes first, then the shapes that stage the links in shared memory
+
+
+def test_every_launch_shape_gives_the_same_fix():
+    """The autotuner may pick any compiled shape.  Shapes of one kernel body compute
+    the same bits; the shared-memory staged body evaluates the same expressions
+    (the compiler may fuse multiply-adds differently), so against the plain body the
+    fix agrees to rounding: the same gauge functional, G to the accuracy e2 allows,
+    the sweep count to one half-sweep."""
     ns, nt = 8, 8
     U0 = gfc.synth_config(ns, nt, 53, 0.5)
     orc.reunitarize(U0)
-    results = {}
     with gfc.Lattice(ns, nt, mixed=True) as lat:
         lat.upload_links(U0, 8, False)
         lat.save_links()
         times = lat.autotune()
         assert all(t > 0 for t in times["exact"] + times["fast64"] + times["fast32"])
         assert lat.download_links().tobytes() == U0.tobytes()   # restored after tuning
-        for kind, n in (("exact", 3), ("fast64", 7), ("fast32", 7)):
-            outs = set()
-            for s in range(n):
+        for kind in ("exact", "fast64", "fast32"):
+            prec = {"exact": gfc.PREC_FP64_EXACT, "fast64": gfc.PREC_FP64_FAST, "fast32": gfc.PREC_MIXED}[kind]
+            runs = []
+            for s in range(len(times[kind])):
                 lat.restore_links()
                 lat.set_shapes(**{kind: s})
-                prec = {"exact": gfc.PREC_FP64_EXACT, "fast64": gfc.PREC_FP64_FAST, "fast32": gfc.PREC_MIXED}[kind]
                 rc, rep = lat.fix(gfc.default_params(tolerance=1e-14),
                                   gfc.options(precision=prec, stop_rule=gfc.STOP_EVERY))
                 assert rc > 0
-                outs.add(orc.sha(lat.download_gt()))
-            results[kind] = outs
-    for kind, outs in results.items():
-        assert len(outs) == 1, kind
+                runs.append((rc, rep.functional, lat.download_gt()))
+            groups = [runs] if kind == "exact" else [runs[:N_PLAIN], runs[N_PLAIN:]]
+            for grp in groups:
+                assert len({orc.sha(G) for _, _, G in grp}) == 1, kind
+            for rc, F, G in runs:
+                assert abs(rc - runs[0][0]) <= 1
+                assert F == pytest.approx(runs[0][1], rel=1e-12)
+                np.testing.assert_allclose(G, runs[0][2], atol=1e-6)
 
 
 def test_slice_blocking_same_results():
