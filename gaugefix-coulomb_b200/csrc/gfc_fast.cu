@@ -58,6 +58,7 @@ struct SweepArgs {
     int hist_n;
     unsigned *stop;     // stop word (0 = keep going); nullptr = never stop
     double tol_sum;     // stop when post(sweep-1) + pre(sweep) <= tol_sum
+    int test;           // 1: hist holds post(sweep-1) of this run, so the stop test applies
     unsigned *status;
 };
 
@@ -170,7 +171,7 @@ __device__ void fused_reduce(const SweepArgs &a, double pre, double post) {
         if (a.stop) atomicExch(a.stop, 0x80000000u | (unsigned)(a.sweep + 1));
         return;
     }
-    if (a.stop && a.sweep >= 1 && a.sweep - 1 < a.hist_n) {
+    if (a.stop && a.test && a.sweep >= 1 && a.sweep - 1 < a.hist_n) {
         double e2 = __ldcg(a.hist + 2 * (a.sweep - 1) + 1) + s0;
         if (e2 <= a.tol_sum) atomicExch(a.stop, (unsigned)(a.sweep + 1));
     }
@@ -412,7 +413,7 @@ static void dispatch_fast(int v, dim3 grid, cudaStream_t st, typename S::V *u, t
 // One half-sweep of timeslices [t0, t0 + nsl) (all slices by default).
 template <class S>
 static void launch_fast(gfc_ctx *c, typename S::V *u, typename S::V *g, int sweep, double omega, unsigned hits,
-                        int track, unsigned *stop, double tol_sum, int t0 = 0, int nsl = -1) {
+                        int track, unsigned *stop, double tol_sum, int t0 = 0, int nsl = -1, int test = 1) {
     const Lat &l = c->lat;
     TrackPtrs tp = track_ptrs(c);
     SweepArgs a{};
@@ -432,6 +433,7 @@ static void launch_fast(gfc_ctx *c, typename S::V *u, typename S::V *g, int swee
     a.hist_n = c->hist_n;
     a.stop = stop;
     a.tol_sum = tol_sum;
+    a.test = test;
     a.status = c->dstatus;
     const int v = sizeof(typename S::T) == 8 ? c->shape_fast64 : c->shape_fast32;
     dispatch_fast<S>(v, dim3(0, nsl < 0 ? l.nt : nsl), c->s, u, g, a);
@@ -552,7 +554,7 @@ static int read_stop(gfc_ctx *c, const unsigned *stop, unsigned *h) {
 // half-sweep late); slice-blocked, the round in progress is completed.
 template <class S>
 static int run_until(gfc_ctx *c, typename S::V *u, typename S::V *g, int sweep0, int max_sweeps, double tol_e2,
-                     double omega, unsigned hits, unsigned reunit, int *done, int *first_below) {
+                     double omega, unsigned hits, unsigned reunit, int dense_check, int *done, int *first_below) {
     const Lat &l = c->lat;
     int rc = ensure_track_buffers(c, max_sweeps + 2);
     if (rc) return rc;
@@ -567,18 +569,48 @@ static int run_until(gfc_ctx *c, typename S::V *u, typename S::V *g, int sweep0,
     unsigned hstop = 0;
     *first_below = -1;
     if (G >= l.nt && K == 1) {
+        // e2 after half-sweep k needs the fused sums of half-sweeps k and k + 1.
+        // While the tolerance is far (by the last measured value and the rate
+        // between the last two measurements) only the last pair of each chunk of 32
+        // is measured; from then on every half-sweep is, so the stop is still at the
+        // first half-sweep whose e2 is below the tolerance.  The measuring costs
+        // about a sixth of a half-sweep's time.
         const int chunk = 32;
+        bool dense = dense_check != 0;
+        bool prev_tracked = false;
+        int k_a = -1;
+        double e2_a = 0.0;
         while (sweep < max_sweeps) {
-            int end = std::min(max_sweeps, sweep + chunk);
+            const int end = std::min(max_sweeps, sweep + chunk);
+            const int first_tracked = dense ? sweep : std::max(sweep, end - 2);
             for (; sweep < end; sweep++) {
-                launch_fast<S>(c, u, g, sweep, omega, hits, 1, tp.stop, tol_sum);
+                const int tr = sweep >= first_tracked;
+                launch_fast<S>(c, u, g, sweep, omega, hits, tr, tp.stop, tol_sum, 0, -1, tr && prev_tracked);
+                prev_tracked = tr;
                 if (reunit && !((sweep + 1) % reunit)) {
                     launch_reunit<S>(c, u, 3 * l.npar, tp.stop);
                     launch_reunit<S>(c, g, l.npar, tp.stop);
                 }
             }
+            const int k = end - 2;   // e2 after half-sweep k is known from this chunk's pair
+            const bool measured = !dense && k >= first_tracked && k + 1 < c->hist_n;
+            if (measured)
+                GFC_CHECK(cudaMemcpyAsync(c->hres + 20, c->e2_hist + 2 * k + 1, 2 * sizeof(double),
+                                          cudaMemcpyDeviceToHost, c->s));
             if ((rc = read_stop(c, tp.stop, &hstop))) return rc;
             if (hstop) break;
+            if (measured) {
+                const double e2 = (c->hres[20] + c->hres[21]) / (double)l.v;   // post(k) + pre(k + 1)
+                if (!(e2 == e2)) break;   // NaN: the status word has it; stop sweeping
+                if (e2 <= 1e3 * tol_e2) {
+                    dense = true;
+                } else if (k_a >= 0 && e2 < e2_a) {
+                    const double rate = pow(e2 / e2_a, 1.0 / (double)(k - k_a));
+                    if (e2 * pow(rate, 2.0 * chunk) <= 10.0 * tol_e2) dense = true;
+                }
+                k_a = k;
+                e2_a = e2;
+            }
         }
         if (hstop & 0x80000000u) {
             set_error("NaN in the gauge functional at half-sweep %u", hstop & 0x7fffffffu);
@@ -636,13 +668,13 @@ int fix_every_sweep(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_r
     if (o->precision == GFC_PREC_FP64_FULL) {
         // plain FP64: full 3x3 storage, same fast arithmetic
         rc = run_until<S64>(c, c->u, c->g, 0, (int)p->max_sweeps_to_fix, tol_e2, (double)p->omega_OR, p->hits,
-                            p->sweeps_to_reunitarization, &done, &below);
+                            p->sweeps_to_reunitarization, o->dense_check, &done, &below);
         if (rc) return rc;
     } else {
         if ((rc = ensure_2row(c))) return rc;
         pack_2row(c);
         rc = run_until<S64R>(c, c->u64r, c->g64r, 0, (int)p->max_sweeps_to_fix, tol_e2, (double)p->omega_OR,
-                             p->hits, p->sweeps_to_reunitarization, &done, &below);
+                             p->hits, p->sweeps_to_reunitarization, o->dense_check, &done, &below);
         if (rc) return rc;
         unpack_2row(c);
     }
@@ -686,7 +718,7 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     const unsigned reunit32 = std::min<unsigned>(p->sweeps_to_reunitarization, 50u);
     int done = 0, below = -1;
     rc = run_until<S32>(c, (float4 *)c->u32, (float4 *)c->g32, 0, (int)p->max_sweeps_to_fix, sw,
-                        (double)p->omega_OR, p->hits, reunit32, &done, &below);
+                        (double)p->omega_OR, p->hits, reunit32, o->dense_check, &done, &below);
     if (rc) return rc;
     r->sweeps_fp32 = done;
     if (below < 0) {
@@ -708,7 +740,7 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     if ((rc = ensure_2row(c))) return rc;
     pack_2row(c);
     rc = run_until<S64R>(c, c->u64r, c->g64r, done, (int)p->max_sweeps_to_fix, tol_e2, (double)p->omega_OR,
-                         p->hits, reunit64, &done64, &below);
+                         p->hits, reunit64, o->dense_check, &done64, &below);
     if (rc) return rc;
     unpack_2row(c);
     GFC_CHECK(cudaEventRecord(c->ev_d, c->s));

@@ -51,6 +51,7 @@ class Options(ctypes.Structure):
         ("switch_e2", ctypes.c_double),
         ("refine_reunit", ctypes.c_uint),
         ("block_threads", ctypes.c_int),
+        ("dense_check", ctypes.c_int),
     ]
 
 

@@ -89,6 +89,10 @@ typedef struct {
     double switch_e2;         /* mixed: leave FP32 when e2 < switch_e2 (default 1e-9) */
     unsigned refine_reunit;   /* mixed: reunitarise every n FP64 half-sweeps (0: use params) */
     int    block_threads;     /* 0: library default / autotuned                      */
+    int    dense_check;       /* GFC_STOP_EVERY on the fast paths: 0 (default) measures e2
+                                 on one pair of half-sweeps per 32 while the measured rate
+                                 says the tolerance is far, then after every half-sweep;
+                                 1 measures after every half-sweep throughout            */
 } gfc_options;
 
 void gfc_options_default(gfc_options *o);

@@ -152,3 +152,23 @@ def test_slice_blocking_same_results():
         lat.restore_links()
         rc2, r2 = lat.fix(p, gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY))
         assert rc2 > 0 and r2.final_residue <= 1e-15
+
+
+@pytest.mark.parametrize("precision", [gfc.PREC_FP64_FAST, gfc.PREC_MIXED, gfc.PREC_FP64_FULL])
+def test_sparse_e2_measurement_stops_at_the_same_half_sweep(precision):
+    """Measuring e2 only on one pair of half-sweeps per chunk while the tolerance is
+    far must not change the stop: same first half-sweep below tolerance, same G."""
+    ns, nt = 8, 12
+    U0 = gfc.synth_config(ns, nt, 57, 0.5)
+    out = {}
+    with gfc.Lattice(ns, nt, mixed=True) as lat:
+        lat.upload_links(U0, 8, False)
+        lat.reunitarize()
+        lat.save_links()
+        for dense in (1, 0):
+            lat.restore_links()
+            rc, rep = lat.fix(gfc.default_params(tolerance=1e-15),
+                              gfc.options(precision=precision, stop_rule=gfc.STOP_EVERY, dense_check=dense))
+            out[dense] = (rc, rep.first_below_tol, rep.sweeps_fp32, orc.sha(lat.download_gt()))
+            assert rep.final_residue <= 1e-15
+    assert out[0] == out[1]
