@@ -56,6 +56,8 @@ def parse_args():
     p.add_argument("--no-precision-form", action="store_true", help="skip the 48^3x96 FP32-input mixed run")
     p.add_argument("--serve-requests", type=int, default=24, help="requests of the serving run (0: skip)")
     p.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrival rate per second")
+    p.add_argument("--batch-mix", default="16x32:32,24x48:32,32x64:32",
+                   help="batch run: comma list of NSxNT:count (default: the 96-config mix)")
     p.add_argument("--only", default="", help="comma list of batch,serve: run just those (no headline line)")
     return p.parse_args()
 
@@ -355,7 +357,6 @@ def run_precision_form(a, gfc):
 
 
 # ----------------------------------------------------- batch and serve --
-BATCH_MIX = [(16, 32)] * 32 + [(24, 48)] * 32 + [(32, 64)] * 32
 SERVE_SIZES = [(16, 32), (24, 48), (32, 64), (48, 96), (64, 128)]
 
 
@@ -368,9 +369,19 @@ def site_updates(b, slot, ns, nt):
     return int(b.slice_sweeps(slot).sum()) * (ns ** 3 // 2)
 
 
+def parse_mix(spec):
+    mix = []
+    for part in spec.split(","):
+        geom, n = part.split(":")
+        ns, nt = (int(x) for x in geom.split("x"))
+        mix += [(ns, nt)] * int(n)
+    return mix
+
+
 def run_batch(a, gfc, torch, precision):
-    """96 configs of three sizes in one batch: every timeslice retires on its own e2."""
-    mix = BATCH_MIX
+    """The 96-config mix (32 each of 16^3x32, 24^3x48, 32^3x64) in one batch: every
+    timeslice retires on its own e2."""
+    mix = parse_mix(a.batch_mix)
     scales = batch_scales(len(mix))
     sites = sum(ns ** 3 * nt for ns, nt in mix)
     big = max(set(mix), key=lambda g: g[0] ** 3 * g[1])

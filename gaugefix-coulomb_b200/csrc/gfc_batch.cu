@@ -38,6 +38,13 @@
 namespace gfc {
 
 enum : int { SS_EMPTY = 0, SS_FP32 = 1, SS_PEND = 2, SS_FP64 = 3, SS_DONE = 4 };
+// e2 of a timeslice after half-sweep c needs the fused sums of its half-sweeps c and
+// c + 1.  While its target (switch threshold or tolerance) is far, a timeslice is
+// measured on own half-sweep counts 30, 31 (mod 32) only; once the last measurement
+// or the rate between the last two puts the target near, after every half-sweep.
+enum : int { MF_NOW = 1, MF_PREV = 2, MF_DENSE = 4 };
+constexpr int MEASURE_PERIOD = 32;
+__host__ __device__ constexpr int measure_at(int c) { return c % MEASURE_PERIOD >= MEASURE_PERIOD - 2; }
 constexpr int BCHUNK = 128;   // sites per work item = threads per CTA of the sweep kernels
 
 struct BSlot {          // device-visible descriptor of one resident lattice
@@ -56,10 +63,14 @@ struct BState {
     int *state;           // [nslices], gid = slot * max_nt + t
     int *sweeps;          // [nslices] half-sweeps applied to the timeslice
     int *listed;          // [nslices] 1 if this round's sweep work lists hold the timeslice
+    int *mflag;           // [nslices] e2 measurement: MF_NOW, MF_PREV, MF_DENSE
+    int *mk;              // [nslices] own half-sweep count of the last e2 measurement (-1: none)
+    double *me2;          // [nslices] that e2
     double *ring;         // [2][nslices][2]: (pre, post) e2 sums of the last two half-sweeps
     int2 *items32, *items64, *pend;
     int cap_items, cap_pend;
     int *counts;          // [0] n32 [1] n64 [2] npend [3] active timeslices [4] half-sweep k [5] overflow
+                          // [6] [7] item cursors [8] [9] FP32 / FP64 reunitarisation due
     unsigned *status;
     double omega, switch_e2, tol;
     unsigned hits, reunit32, reunit64;
@@ -180,6 +191,8 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
     const int expect = F64 ? SS_FP64 : SS_FP32;
     const int2 *items = F64 ? b.items64 : b.items32;
     int *cursor = b.counts + (F64 ? 7 : 6);
+    // the previous half-sweep's reunitarisation flags have been consumed
+    if (!F64 && blockIdx.x == 0 && threadIdx.x == 0) b.counts[8] = b.counts[9] = 0;
     // Items come one at a time from a shared cursor, so a CTA held up by a
     // timeslice's final reduction does not hold back a fixed share of the list.
     // Thread 0 asks for item j + 1 while item j is processed and publishes it in
@@ -197,6 +210,7 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
         // a timeslice retired earlier in this round still has items in the list;
         // the state is the same for every thread of the CTA
         if (*(volatile int *)&b.state[gid] == expect) {
+            const int track = b.mflag[gid] & MF_NOW;   // the same for every thread of the CTA
             const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
             const BSlot &sl = b.slots[slot];
             const Lat l = sl.l;
@@ -207,28 +221,31 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
             double pre = 0.0, post = 0.0;
             if (off < vsh) {
                 if constexpr (STG)
-                    fast_site_staged<S, BCHUNK, false>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, 1,
-                                                       pre, post, (typename S::V *)bstage);
+                    fast_site_staged<S, BCHUNK, false>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits,
+                                                       track, pre, post, (typename S::V *)bstage);
                 else
-                    fast_site<S>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, 1, pre, post);
+                    fast_site<S>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, track, pre, post);
             }
-            // chunk partials (deterministic order inside the block)
             // the chunk's partials; k_bslice combines them after the half-sweep
-            block_pair_sum(pre, post, sh);
-            if (threadIdx.x == 0) {
-                double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
-                pp[0] = pre;
-                pp[1] = post;
+            if (track) {
+                block_pair_sum(pre, post, sh);
+                if (threadIdx.x == 0) {
+                    double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
+                    pp[0] = pre;
+                    pp[1] = post;
+                }
             }
         }
         if (threadIdx.x == 0) next[(j + 1) & 1] = ahead;
     }
 }
 
-// After both sweep kernels of a half-sweep: one warp per swept timeslice sums its
-// chunk partials in a fixed order (lane-strided, then a shuffle tree), records the
-// timeslice's e2 after k half-sweeps and retires it: FP32 -> pending switch at the
-// switch threshold, FP64 -> done at the tolerance, NaN -> done with the status bit.
+// After both sweep kernels of a half-sweep, one warp per swept timeslice: advances its
+// half-sweep count and e2 measurement schedule; where the half-sweep was measured,
+// sums the chunk partials in a fixed order (lane-strided, then a shuffle tree) and,
+// with the previous half-sweep measured too, has the timeslice's e2 after the
+// previous half-sweep and retires it: FP32 -> pending switch at the switch
+// threshold, FP64 -> done at the tolerance, NaN -> done with the status bit.
 __global__ void k_bslice(BState b) {
     const int lane = threadIdx.x & 31;
     const int k = b.counts[4];
@@ -238,34 +255,60 @@ __global__ void k_bslice(BState b) {
         // swept in this half-sweep: listed at the round's start and not retired since
         // (a timeslice switched to FP64 at the start of the round has no items yet)
         if (!b.listed[gid] || (st != SS_FP32 && st != SS_FP64)) continue;   // uniform in the warp
+        const int f = b.mflag[gid];
+        const int c = b.sweeps[gid];   // this half-sweep's own index
         const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
         const BSlot &sl = b.slots[slot];
-        const double *pp = sl.part + (size_t)t * sl.nbx * 2;
         double s0 = 0.0, s1 = 0.0;
-        for (int q = lane; q < sl.nbx; q += 32) {
-            s0 += pp[2 * q];
-            s1 += pp[2 * q + 1];
-        }
+        if (f & MF_NOW) {
+            const double *pp = sl.part + (size_t)t * sl.nbx * 2;
+            for (int q = lane; q < sl.nbx; q += 32) {
+                s0 += pp[2 * q];
+                s1 += pp[2 * q + 1];
+            }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            s0 += __shfl_down_sync(0xffffffffu, s0, o);
-            s1 += __shfl_down_sync(0xffffffffu, s1, o);
+            for (int o = 16; o > 0; o >>= 1) {
+                s0 += __shfl_down_sync(0xffffffffu, s0, o);
+                s1 += __shfl_down_sync(0xffffffffu, s1, o);
+            }
         }
-        if (lane == 0) {
+        if (lane != 0) continue;
+        int nf = f & MF_DENSE;
+        int nst = st;
+        if (f & MF_NOW) {
             double *rprev = b.ring + ((size_t)((k + 1) & 1) * b.nslices + gid) * 2;
             double *rcur = b.ring + ((size_t)(k & 1) * b.nslices + gid) * 2;
-            const double e2s = (s0 + rprev[1]) / (double)sl.l.vs;   // e2 of the timeslice after k half-sweeps
             rcur[0] = s0;
             rcur[1] = s1;
-            b.sweeps[gid] += 1;
             if (!(s0 == s0) || !(s1 == s1)) {
                 atomicOr(b.status, GFC_STATUS_NAN);
-                b.state[gid] = SS_DONE;
-            } else if (st == SS_FP32 && e2s <= b.switch_e2) {
-                b.state[gid] = SS_PEND;
-            } else if (st == SS_FP64 && e2s <= b.tol) {
-                b.state[gid] = SS_DONE;
+                nst = SS_DONE;
+            } else if (f & MF_PREV) {
+                const double e2s = (s0 + rprev[1]) / (double)sl.l.vs;   // e2 after half-sweep c - 1
+                const double target = st == SS_FP32 ? b.switch_e2 : b.tol;
+                if (e2s <= target) {
+                    nst = st == SS_FP32 ? SS_PEND : SS_DONE;
+                } else if (!(nf & MF_DENSE)) {
+                    if (e2s <= 1e3 * target) {
+                        nf |= MF_DENSE;
+                    } else if (b.mk[gid] >= 0 && e2s < b.me2[gid]) {
+                        const double rate = pow(e2s / b.me2[gid], 1.0 / (double)(c - 1 - b.mk[gid]));
+                        if (e2s * pow(rate, 2.0 * MEASURE_PERIOD) <= 10.0 * target) nf |= MF_DENSE;
+                    }
+                }
+                b.mk[gid] = c - 1;
+                b.me2[gid] = e2s;
             }
+            nf |= MF_PREV;
+        }
+        if ((nf & MF_DENSE) || measure_at(c + 1)) nf |= MF_NOW;
+        b.mflag[gid] = nf;
+        b.sweeps[gid] = c + 1;
+        if (nst != st) {
+            b.state[gid] = nst;
+        } else {
+            const unsigned period = st == SS_FP32 ? b.reunit32 : b.reunit64;
+            if (period && (unsigned)(c + 1) % period == 0) b.counts[st == SS_FP32 ? 8 : 9] = 1;
         }
     }
 }
@@ -284,7 +327,7 @@ __global__ void k_btick(BState b) {
 template <class S>
 __global__ void __launch_bounds__(BCHUNK) k_breunit(BState b, unsigned period) {
     constexpr bool F64 = sizeof(typename S::T) == 8;
-    if (period == 0) return;
+    if (period == 0 || !b.counts[F64 ? 9 : 8]) return;   // no timeslice is due this half-sweep
     __shared__ int due[BCHUNK];
     __shared__ int ndue;
     const int n = b.counts[F64 ? 1 : 0];
@@ -386,6 +429,8 @@ __global__ void k_switch_done(BState b) {
     b.state[gid] = SS_FP64;
     b.ring[((size_t)0 * b.nslices + gid) * 2 + 1] = __longlong_as_double(0x7ff0000000000000LL);
     b.ring[((size_t)1 * b.nslices + gid) * 2 + 1] = __longlong_as_double(0x7ff0000000000000LL);
+    b.mflag[gid] = measure_at(b.sweeps[gid]) ? MF_NOW : 0;   // a new target: measure afresh
+    b.mk[gid] = -1;
 }
 
 // activate the timeslices of one slot in `state`
@@ -395,6 +440,8 @@ __global__ void k_activate(BState b, int gid0, int nt, int state) {
     const int gid = gid0 + t;
     b.state[gid] = state;
     b.sweeps[gid] = 0;
+    b.mflag[gid] = measure_at(0) ? MF_NOW : 0;
+    b.mk[gid] = -1;
     for (int q = 0; q < 2; q++) {
         b.ring[((size_t)q * b.nslices + gid) * 2] = 0.0;
         b.ring[((size_t)q * b.nslices + gid) * 2 + 1] = __longlong_as_double(0x7ff0000000000000LL);
@@ -420,7 +467,8 @@ struct gfc_batch {
     std::vector<void *> mem;        // per-slot allocation
     std::vector<int> used, ns, nt, activated;
     BSlot *dslots = nullptr;
-    int *state = nullptr, *sweeps = nullptr, *counts = nullptr, *listed = nullptr;
+    int *state = nullptr, *sweeps = nullptr, *counts = nullptr, *listed = nullptr, *mflag = nullptr, *mk = nullptr;
+    double *me2 = nullptr;
     double *ring = nullptr;
     int2 *items32 = nullptr, *items64 = nullptr, *pend = nullptr;
     int cap_items = 0, cap_pend = 0;
@@ -480,13 +528,17 @@ extern "C" int gfc_batch_create(int device, size_t max_sites, int max_slots, int
     BTRY(cudaMalloc(&b->sweeps, sizeof(int) * b->nslices));
     BTRY(cudaMalloc(&b->listed, sizeof(int) * b->nslices));
     BTRY(cudaMemset(b->listed, 0, sizeof(int) * b->nslices));
+    BTRY(cudaMalloc(&b->mflag, sizeof(int) * b->nslices));
+    BTRY(cudaMemset(b->mflag, 0, sizeof(int) * b->nslices));
+    BTRY(cudaMalloc(&b->mk, sizeof(int) * b->nslices));
+    BTRY(cudaMalloc(&b->me2, sizeof(double) * b->nslices));
     BTRY(cudaMemset(b->sweeps, 0, sizeof(int) * b->nslices));
     BTRY(cudaMalloc(&b->ring, sizeof(double) * 4 * b->nslices));
     BTRY(cudaMalloc(&b->items32, sizeof(int2) * b->cap_items));
     BTRY(cudaMalloc(&b->items64, sizeof(int2) * b->cap_items));
     BTRY(cudaMalloc(&b->pend, sizeof(int2) * b->cap_pend));
-    BTRY(cudaMalloc(&b->counts, sizeof(int) * 8));
-    BTRY(cudaMemset(b->counts, 0, sizeof(int) * 8));
+    BTRY(cudaMalloc(&b->counts, sizeof(int) * 16));
+    BTRY(cudaMemset(b->counts, 0, sizeof(int) * 16));
     BTRY(cudaMalloc(&b->status, sizeof(unsigned)));
     BTRY(cudaMemset(b->status, 0, sizeof(unsigned)));
     BTRY(cudaMallocHost(&b->hcounts, sizeof(int) * 8));
@@ -530,6 +582,9 @@ extern "C" int gfc_batch_destroy(gfc_batch *b) {
     cudaFree(b->state);
     cudaFree(b->sweeps);
     cudaFree(b->listed);
+    cudaFree(b->mflag);
+    cudaFree(b->mk);
+    cudaFree(b->me2);
     cudaFree(b->ring);
     cudaFree(b->items32);
     cudaFree(b->items64);
@@ -720,6 +775,8 @@ extern "C" int gfc_batch_activate(gfc_batch *b, int slot, int precision) {
     bs.state = b->state;
     bs.sweeps = b->sweeps;
     bs.ring = b->ring;
+    bs.mflag = b->mflag;
+    bs.mk = b->mk;
     k_activate<<<(l.nt + 127) / 128, 128, 0, b->s>>>(bs, slot * b->max_nt, l.nt, st);
     b->launches += 5;
     b->activated[slot] = 1;
@@ -736,6 +793,9 @@ static BState make_state(gfc_batch *b, const gfc_params *p, const gfc_options *o
     s.state = b->state;
     s.sweeps = b->sweeps;
     s.listed = b->listed;
+    s.mflag = b->mflag;
+    s.mk = b->mk;
+    s.me2 = b->me2;
     s.ring = b->ring;
     s.items32 = b->items32;
     s.items64 = b->items64;
