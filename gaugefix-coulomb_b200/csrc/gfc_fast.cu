@@ -75,9 +75,10 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 // and, with sg, G are copied to shared memory by cp.async before the update
 // (6 or 7 x 96 B per thread in FP64, 48 B in FP32), which also bounds residency.
 struct SShape {
-    int block, minb, sg;
+    int block, minb, sg, nst;   // nst: links staged per site (whole directions: 2, 4 or 6)
 };
-constexpr SShape kStaged[] = {{128, 2, 1}, {64, 5, 1}, {128, 3, 0}, {256, 1, 1}, {128, 4, 1}, {128, 5, 1}};
+constexpr SShape kStaged[] = {{128, 2, 1, 6}, {64, 5, 1, 6}, {128, 3, 0, 6}, {256, 1, 1, 6}, {128, 4, 1, 6},
+                              {128, 5, 1, 6}, {128, 4, 0, 4}, {64, 6, 0, 4}, {128, 5, 0, 2}};
 constexpr int kNumStaged = sizeof(kStaged) / sizeof(kStaged[0]);
 constexpr int kNumAll = kNumShapes + kNumStaged;   // shape indices: plain, then staged
 static_assert(3 + 2 * kNumAll + 8 == GFC_TUNE_SLOTS, "autotune time slots");
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_fast(typename S::V *__res
     if (a.track) fused_reduce<BLOCK>(a, pre, post);
 }
 
-template <class S, int BLOCK, int MINB, bool SG>
+template <class S, int BLOCK, int MINB, bool SG, int NST>
 __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_staged(typename S::V *__restrict__ u,
                                                               typename S::V *__restrict__ g, SweepArgs a) {
     extern __shared__ __align__(16) unsigned char staged_smem[];
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_staged(typename S::V *__r
     const uint32_t off = blockIdx.x * BLOCK + threadIdx.x;
     double pre = 0.0, post = 0.0;
     if (off < vsh)
-        fast_site_staged<S, BLOCK, SG>(u, g, l, a.par, (a.t0 + blockIdx.y) * vsh + off, (T)a.omega, a.hits, a.track,
+        fast_site_staged<S, BLOCK, SG, NST>(u, g, l, a.par, (a.t0 + blockIdx.y) * vsh + off, (T)a.omega, a.hits, a.track,
                                        pre, post, (typename S::V *)staged_smem);
     if (a.track) fused_reduce<BLOCK>(a, pre, post);
 }
@@ -358,16 +359,16 @@ static void launch_shape(dim3 grid, cudaStream_t st, typename S::V *u, typename 
 }
 
 template <class S>
-static constexpr size_t staged_bytes(int block, int sg) {
-    return (size_t)(6 + sg) * S::NS * block * 16;
+static constexpr size_t staged_bytes(int block, int sg, int nst) {
+    return (size_t)(nst + sg) * S::NS * block * 16;
 }
 
 template <class S, int K>
 static void launch_staged(dim3 grid, cudaStream_t st, typename S::V *u, typename S::V *g, const SweepArgs &a) {
     constexpr SShape sh = kStaged[K];
-    constexpr size_t bytes = staged_bytes<S>(sh.block, sh.sg);
+    constexpr size_t bytes = staged_bytes<S>(sh.block, sh.sg, sh.nst);
     static_assert(bytes <= 227 * 1024, "staged tile exceeds shared memory");
-    auto kern = k_sweep_staged<S, sh.block, sh.minb, (bool)sh.sg>;
+    auto kern = k_sweep_staged<S, sh.block, sh.minb, (bool)sh.sg, sh.nst>;
     // the attribute is set once per device (a CUDA function attribute is per context)
     static unsigned long long done = 0;
     int dev = 0;
@@ -392,6 +393,9 @@ static void dispatch_fast(int v, dim3 grid, cudaStream_t st, typename S::V *u, t
             case 3: return launch_staged<S, 3>(grid, st, u, g, a);
             case 4: return launch_staged<S, 4>(grid, st, u, g, a);
             case 5: return launch_staged<S, 5>(grid, st, u, g, a);
+            case 6: return launch_staged<S, 6>(grid, st, u, g, a);
+            case 7: return launch_staged<S, 7>(grid, st, u, g, a);
+            case 8: return launch_staged<S, 8>(grid, st, u, g, a);
             default: break;
         }
     } else if (v >= kNumShapes) {
@@ -758,8 +762,8 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
 // and keeps the fastest per kernel.  The links are saved first and restored after
 // (the timed half-sweeps change them), and G is reset to the identity.
 // times (optional, length >= GFC_TUNE_SLOTS) receives seconds per half-sweep:
-//   [0..2] exact shapes, [3..17] FP64 fast shapes (9 plain, then 6 staged), [18..32]
-//   FP32 shapes, [33..36] FP64 slice blocking, [37..40] FP32 slice blocking (0: not timed).
+//   [0..2] exact shapes, [3..20] FP64 fast shapes (9 plain, then 9 staged), [21..38]
+//   FP32 shapes, [39..42] FP64 slice blocking, [43..46] FP32 slice blocking (0: not timed).
 using namespace gfc;
 
 extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {

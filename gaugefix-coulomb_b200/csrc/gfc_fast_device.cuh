@@ -555,13 +555,14 @@ __device__ __forceinline__ void apply_staged(const typename S::V *src, int sst, 
     }
 }
 
-// fast_site with the six links (and, with SG, G) first copied into shared memory
-// by cp.async: every byte the site needs is requested at once, without registers
-// held for it, and the link update reads its operands back from shared memory
-// instead of from L2.  Staged layout per CTA: entry e of matrix m of thread x at
-// sm[(m * NS + e) * BLOCK + x] (m = 2d forward, 2d+1 backward link of direction d,
-// m = 6 G).  Two-row storage only.
-template <class S, int BLOCK, bool SG>
+// fast_site with the links of the first NST / 2 directions (and, with SG, G) first
+// copied into shared memory by cp.async: those bytes are requested at once, without
+// registers held for them, and the link update reads them back from shared memory
+// instead of from L2 (the links of the other directions are loaded from global
+// memory twice, as in fast_site).  Staged layout per CTA: entry e of matrix m of
+// thread x at sm[(m * NS + e) * BLOCK + x] (m = 2d forward, 2d+1 backward link of
+// direction d, m = NST for G).  Two-row storage only.
+template <class S, int BLOCK, bool SG, int NST = 6>
 __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, typename S::V *__restrict__ g,
                                                  const Lat &l, int par, uint32_t i, typename S::T omega,
                                                  unsigned hits, int track, double &pre, double &post,
@@ -575,9 +576,11 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
     uint32_t ib[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) ib[d] = back_L(l, c, d) >> 1;
+    static_assert(NST == 2 || NST == 4 || NST == 6, "whole directions are staged");
+    constexpr int ND = NST / 2;   // staged directions
     V *my = sm + threadIdx.x;
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
+    for (int d = 0; d < ND; d++) {
         const V *f = u + su_idx<S>(l, d, par, i);
         const V *r = u + su_idx<S>(l, d, op, ib[d]);
 #pragma unroll
@@ -589,7 +592,7 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
     if (SG) {
         const V *gp = g + sg_idx<S>(l, par, i);
 #pragma unroll
-        for (int e = 0; e < S::NS; e++) cp_async16(my + (6 * S::NS + e) * BLOCK, gp + (size_t)e * l.vh);
+        for (int e = 0; e < S::NS; e++) cp_async16(my + (NST * S::NS + e) * BLOCK, gp + (size_t)e * l.vh);
     }
     cp_async_wait_all();
 
@@ -599,8 +602,13 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         Mt<T> f, r;
-        S::load(my + (2 * d) * S::NS * BLOCK, BLOCK, f);
-        S::load(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, r);
+        if (d < ND) {
+            S::load(my + (2 * d) * S::NS * BLOCK, BLOCK, f);
+            S::load(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, r);
+        } else {
+            S::load(u + su_idx<S>(l, d, par, i), l.vh, f);
+            S::load(u + su_idx<S>(l, d, op, ib[d]), l.vh, r);
+        }
 #pragma unroll
         for (int x = 0; x < 3; x++)
 #pragma unroll
@@ -616,7 +624,7 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
     {
         Mt<T> m, o;
         if (SG)
-            S::load(my + 6 * S::NS * BLOCK, BLOCK, m);
+            S::load(my + NST * S::NS * BLOCK, BLOCK, m);
         else
             S::load(g + sg_idx<S>(l, par, i), l.vh, m);
         fprod_left<S>(up, m, o);
@@ -625,9 +633,15 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
     double cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        apply_staged<S, true>(my + (2 * d) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, par, i), l.vh, up, track, cc);
-        apply_staged<S, false>(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, op, ib[d]), l.vh, up,
-                               track, cc);
+        if (d < ND) {
+            apply_staged<S, true>(my + (2 * d) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, par, i), l.vh, up, track,
+                                  cc);
+            apply_staged<S, false>(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, op, ib[d]), l.vh,
+                                   up, track, cc);
+        } else {
+            apply_forward<S>(u + su_idx<S>(l, d, par, i), l.vh, up, track, cc);
+            apply_backward<S>(u + su_idx<S>(l, d, op, ib[d]), l.vh, up, track, cc);
+        }
     }
     if (track) {
         cc[7] *= 0.57735026918962576451;

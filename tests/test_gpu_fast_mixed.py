@@ -86,15 +86,17 @@ def test_fast_tracks_exact_per_sweep():
     assert out[gfc.PREC_FP64_FAST][1] == pytest.approx(out[gfc.PREC_FP64_EXACT][1], rel=1e-12)
 
 
-N_PLAIN = 9   # plain shapes first, then the shapes that stage the links in shared memory
+# shape indices by kernel body: plain, all six links staged in shared memory, four
+# staged, two staged (gfc_ctx_autotune's order)
+BODIES = [range(0, 9), range(9, 15), range(15, 17), range(17, 18)]
 
 
 def test_every_launch_shape_gives_the_same_fix():
     """The autotuner may pick any compiled shape.  Shapes of one kernel body compute
-    the same bits; the shared-memory staged body evaluates the same expressions
-    (the compiler may fuse multiply-adds differently), so against the plain body the
-    fix agrees to rounding: the same gauge functional, G to the accuracy e2 allows,
-    the sweep count to one half-sweep."""
+    the same bits; the shared-memory staged bodies evaluate the same expressions
+    (the compiler may fuse multiply-adds differently), so across bodies the fix
+    agrees to rounding: the same gauge functional, G to the accuracy e2 allows, the
+    sweep count to one half-sweep."""
     ns, nt = 8, 8
     U0 = gfc.synth_config(ns, nt, 53, 0.5)
     orc.reunitarize(U0)
@@ -114,7 +116,8 @@ def test_every_launch_shape_gives_the_same_fix():
                                   gfc.options(precision=prec, stop_rule=gfc.STOP_EVERY))
                 assert rc > 0
                 runs.append((rc, rep.functional, lat.download_gt()))
-            groups = [runs] if kind == "exact" else [runs[:N_PLAIN], runs[N_PLAIN:]]
+            groups = [runs] if kind == "exact" else [[runs[i] for i in body] for body in BODIES]
+            assert kind == "exact" or sum(len(b) for b in BODIES) == len(runs)
             for grp in groups:
                 assert len({orc.sha(G) for _, _, G in grp}) == 1, kind
             for rc, F, G in runs:
