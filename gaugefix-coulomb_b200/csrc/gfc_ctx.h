@@ -42,9 +42,11 @@ struct gfc_ctx {
     long long launches = 0;
     // launch shapes of the sweep kernels (indices into the compiled shape tables;
     // defaults until gfc_ctx_autotune measures them for this lattice)
-    int shape_exact = 1;
-    int shape_fast64 = 1;
-    int shape_fast32 = 2;
+    // (the defaults are the shapes measured fastest at 32^3x64 on a B200: exact with
+    // staged links 128x2, fast FP64 staged 128x3, FP32 plain 128x5)
+    int shape_exact = 3;
+    int shape_fast64 = 11;
+    int shape_fast32 = 7;
     int tuned = 0;
     // slice blocking of the fast sweeps: groups of blk*_slices timeslices run
     // blk*_sweeps half-sweeps each while resident in L2 (0 / 1: not blocked)

@@ -81,7 +81,8 @@ constexpr SShape kStaged[] = {{128, 2, 1, 6}, {64, 5, 1, 6}, {128, 3, 0, 6}, {25
                               {128, 5, 1, 6}, {128, 4, 0, 4}, {64, 6, 0, 4}, {128, 5, 0, 2}};
 constexpr int kNumStaged = sizeof(kStaged) / sizeof(kStaged[0]);
 constexpr int kNumAll = kNumShapes + kNumStaged;   // shape indices: plain, then staged
-static_assert(3 + 2 * kNumAll + 8 == GFC_TUNE_SLOTS, "autotune time slots");
+constexpr int kNE = 5;   // exact-kernel shapes (gfc_kernels_exact.cu)
+static_assert(kNE + 2 * kNumAll + 8 == GFC_TUNE_SLOTS, "autotune time slots");
 constexpr int MIN_BLOCK = 64;   // smallest block: sizes the per-block partial buffers
 
 // deterministic sum of NQ values over the block; result in thread 0
@@ -762,8 +763,8 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
 // and keeps the fastest per kernel.  The links are saved first and restored after
 // (the timed half-sweeps change them), and G is reset to the identity.
 // times (optional, length >= GFC_TUNE_SLOTS) receives seconds per half-sweep:
-//   [0..2] exact shapes, [3..20] FP64 fast shapes (9 plain, then 9 staged), [21..38]
-//   FP32 shapes, [39..42] FP64 slice blocking, [43..46] FP32 slice blocking (0: not timed).
+//   [0..4] exact shapes, [5..22] FP64 fast shapes (9 plain, then 9 staged), [23..40]
+//   FP32 shapes, [41..44] FP64 slice blocking, [45..48] FP32 slice blocking (0: not timed).
 using namespace gfc;
 
 extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
@@ -816,7 +817,7 @@ extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
     };
     if (which & 1) {
         double best = 1e30;
-        for (int s = 0; s < exact_num_shapes(); s++) {
+        for (int s = 0; s < kNE && s < exact_num_shapes(); s++) {
             double t = timed([&](int k) { launch_sweep_exact(c->u, c->g, l, k, 1.95, 2, c->s, s); });
             times[s] = t;
             if (t < best) {
@@ -832,7 +833,7 @@ extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
         for (int v = 0; v < kNumAll; v++) {
             double t = timed(
                 [&](int k) { dispatch_fast<S64R>(v, dim3(0, l.nt), c->s, c->u64r, c->g64r, args_for(k)); });
-            times[3 + v] = t;
+            times[kNE + v] = t;
             if (t < best) {
                 best = t;
                 c->shape_fast64 = v;
@@ -848,7 +849,7 @@ extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
             double t = timed([&](int k) {
                 dispatch_fast<S32>(v, dim3(0, l.nt), c->s, (float4 *)c->u32, (float4 *)c->g32, args_for(k));
             });
-            times[3 + kNumAll + v] = t;
+            times[kNE + kNumAll + v] = t;
             if (t < best) {
                 best = t;
                 c->shape_fast32 = v;
@@ -894,17 +895,17 @@ extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
     if (which & 2) {
         double base = 1e30;
         for (int v = 0; v < kNumAll; v++)
-            if (times[3 + v] > 0 && times[3 + v] < base) base = times[3 + v];
+            if (times[kNE + v] > 0 && times[kNE + v] < base) base = times[kNE + v];
         rc = tune_blocking(S64R{}, c->u64r, c->g64r, 96, c->blk64_slices, c->blk64_sweeps, base,
-                           times + 3 + 2 * kNumAll);
+                           times + kNE + 2 * kNumAll);
         if (rc) return rc;
     }
     if ((which & 4) && c->u32 && c->g32) {
         double base = 1e30;
         for (int v = 0; v < kNumAll; v++)
-            if (times[3 + kNumAll + v] > 0 && times[3 + kNumAll + v] < base) base = times[3 + kNumAll + v];
+            if (times[kNE + kNumAll + v] > 0 && times[kNE + kNumAll + v] < base) base = times[kNE + kNumAll + v];
         rc = tune_blocking(S32{}, (float4 *)c->u32, (float4 *)c->g32, 48, c->blk32_slices, c->blk32_sweeps, base,
-                           times + 7 + 2 * kNumAll);
+                           times + kNE + 4 + 2 * kNumAll);
         if (rc) return rc;
     }
     GFC_CHECK(cudaGetLastError());

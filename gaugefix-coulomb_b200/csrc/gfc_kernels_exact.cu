@@ -72,6 +72,98 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_exact(double2 *__restrict
     site_update_exact<true>(u, g, l, par, c, omega, hits);
 }
 
+// The same update with the six links first copied into shared memory by cp.async
+// (9 x 16 B per link per thread: the whole site's links requested at once, no
+// registers held for them), read back from there for the link update instead of
+// being loaded again.  Arithmetic and order are those of site_update_exact.
+// Staged layout: entry e of link m of thread x at sm[(m * 9 + e) * BLOCK + x],
+// m = 2d forward, 2d+1 backward link of direction d.
+template <int BLOCK>
+__device__ __forceinline__ void site_update_exact_staged(double2 *__restrict__ u, double2 *__restrict__ g,
+                                                         const Lat &l, int par, const Coord &c, double omega,
+                                                         unsigned hits, double2 *sm) {
+    const int op = par ^ 1;
+    const uint32_t si = c.L >> 1;
+    uint32_t ib[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) ib[d] = back_L(l, c, d) >> 1;
+    double2 *my = sm + threadIdx.x;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double2 *f = u + uidx(l, d, par, 0, si);
+        const double2 *r = u + uidx(l, d, op, 0, ib[d]);
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            const unsigned sf = (unsigned)__cvta_generic_to_shared(my + ((2 * d) * 9 + e) * BLOCK);
+            const unsigned sr = (unsigned)__cvta_generic_to_shared(my + ((2 * d + 1) * 9 + e) * BLOCK);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sf), "l"(f + (size_t)e * l.vh) : "memory");
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sr), "l"(r + (size_t)e * l.vh) : "memory");
+        }
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+
+    M3 w;
+#pragma unroll
+    for (int k = 0; k < 9; k++) w.e[k] = cz();
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        M3 f, r;
+        load_m(my + (2 * d) * 9 * BLOCK, BLOCK, f);
+        load_m(my + (2 * d + 1) * 9 * BLOCK, BLOCK, r);
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++)
+                w.e[EL(a, b)] = xcadd(w.e[EL(a, b)], xcadd(f.e[EL(a, b)], cconj(r.e[EL(b, a)])));
+    }
+
+    M3 upd;
+    xor_update(w, omega, hits, upd);
+    asm volatile("" ::: "memory");   // read the links again from shared memory below
+
+    M3 m, t;
+    load_m(g + gidx(l, par, 0, si), l.vh, m);
+    xprod(upd, m, t);
+    store_m(g + gidx(l, par, 0, si), l.vh, t);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        load_m(my + (2 * d) * 9 * BLOCK, BLOCK, m);
+        xprod(upd, m, t);
+        store_m(u + uidx(l, d, par, 0, si), l.vh, t);
+        load_m(my + (2 * d + 1) * 9 * BLOCK, BLOCK, m);
+        xprod_dag(m, upd, t);
+        store_m(u + uidx(l, d, op, 0, ib[d]), l.vh, t);
+    }
+}
+
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_sweep_exact_staged(double2 *__restrict__ u,
+                                                                    double2 *__restrict__ g, Lat l, int par,
+                                                                    double omega, unsigned hits) {
+    extern __shared__ __align__(16) unsigned char exact_stage[];
+    uint32_t i = blockIdx.x * BLOCK + threadIdx.x;
+    if (i >= l.vh) return;
+    Coord c = coord_cb(l, par, i);
+    site_update_exact_staged<BLOCK>(u, g, l, par, c, omega, hits, (double2 *)exact_stage);
+}
+
+template <int BLOCK, int MINB>
+static void launch_exact_staged(const Lat &l, double2 *u, double2 *g, int par, double omega, unsigned hits,
+                                cudaStream_t s) {
+    constexpr size_t bytes = (size_t)6 * 9 * BLOCK * sizeof(double2);
+    static_assert(bytes <= 227 * 1024, "staged links exceed shared memory");
+    auto kern = k_sweep_exact_staged<BLOCK, MINB>;
+    static unsigned long long done = 0;   // attribute set once per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !(done >> dev & 1ull)) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+        done |= 1ull << dev;
+    }
+    kern<<<(l.vh + BLOCK - 1) / BLOCK, BLOCK, bytes, s>>>(u, g, l, par, omega, hits);
+}
+
 // Odd ns: same-parity sites meet across the periodic boundary, so updates inside
 // a timeslice depend on their order.  One thread per timeslice visits the slice in
 // the reference's z, y, x order; distinct timeslices share no spatial link.
@@ -86,7 +178,7 @@ __global__ void k_sweep_exact_serial(double2 *__restrict__ u, double2 *__restric
     }
 }
 
-int exact_num_shapes() { return 3; }
+int exact_num_shapes() { return 5; }
 
 void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
                         cudaStream_t s, int shape) {
@@ -98,6 +190,12 @@ void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double 
                 break;
             case 2:
                 k_sweep_exact<64, 4><<<(l.vh + 63) / 64, 64, 0, s>>>(u, g, l, par, omega, hits);
+                break;
+            case 3:   // 110.6 KiB of staged links per CTA, 2 CTAs per SM
+                launch_exact_staged<128, 2>(l, u, g, par, omega, hits, s);
+                break;
+            case 4:   // 55.3 KiB per CTA, 4 CTAs per SM
+                launch_exact_staged<64, 4>(l, u, g, par, omega, hits, s);
                 break;
             default:
                 k_sweep_exact<128, 1><<<(l.vh + 127) / 128, 128, 0, s>>>(u, g, l, par, omega, hits);

@@ -287,10 +287,10 @@ class Lattice:
     def autotune(self, which=0):
         """Time every compiled launch shape on this lattice; keep the fastest.
         Returns seconds per half-sweep: {"exact": [...], "fast64": [...], "fast32": [...]}."""
-        t = np.zeros(47)
+        t = np.zeros(49)
         _check(lib.gfc_ctx_autotune(self.h, which, t.ctypes.data), "autotune")
-        return {"exact": t[0:3].tolist(), "fast64": t[3:21].tolist(), "fast32": t[21:39].tolist(),
-                "fast64_blocked": t[39:43].tolist(), "fast32_blocked": t[43:47].tolist()}
+        return {"exact": t[0:5].tolist(), "fast64": t[5:23].tolist(), "fast32": t[23:41].tolist(),
+                "fast64_blocked": t[41:45].tolist(), "fast32_blocked": t[45:49].tolist()}
 
     def set_blocking(self, precision_bits, slices, sweeps):
         _check(lib.gfc_ctx_set_blocking(self.h, precision_bits, slices, sweeps), "set_blocking")

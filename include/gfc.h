@@ -193,13 +193,14 @@ int  gfc_ctx_finalize_temporal(gfc_ctx *c);
  * which: bit 0 exact FP64, bit 1 fast FP64, bit 2 FP32 (0 = all).  The links are
  * saved and restored around the timing (a device copy of all links is kept) and G
  * is reset to the identity.  times (may be NULL) receives seconds per half-sweep:
- * [0..2] exact shapes, [3..20] fast FP64 shapes (9 plain, then 9 with links staged
- * in shared memory by cp.async), [21..38] FP32 shapes (same order), [39..42] fast
- * FP64 slice-blocked candidates, [43..46] FP32 slice-blocked candidates.  Slice
+ * [0..4] exact shapes (3 plain, 2 with the links staged in shared memory), [5..22]
+ * fast FP64 shapes (9 plain, then 9 with links staged in shared memory by cp.async),
+ * [23..40] FP32 shapes (same order), [41..44] fast FP64 slice-blocked candidates,
+ * [45..48] FP32 slice-blocked candidates.  Slice
  * blocking runs a group of timeslices for several half-sweeps while its links stay in
  * L2 (timeslices share no link during the sweeps); it is kept only where it measured
  * faster. */
-#define GFC_TUNE_SLOTS 47
+#define GFC_TUNE_SLOTS 49
 int  gfc_ctx_autotune(gfc_ctx *c, int which, double *times);
 int  gfc_ctx_get_shapes(const gfc_ctx *c, int *exact, int *fast64, int *fast32);
 /* -1 keeps the current choice */
