@@ -46,6 +46,36 @@ template <typename C>
 __device__ __forceinline__ C fconj(C a) {
     return mkc<C>(a.x, -a.y);
 }
+// s + a b and s + a conj(b)
+template <typename C>
+__device__ __forceinline__ C fmac(C s, C a, C b) {
+    return fadd(s, fmul(a, b));
+}
+template <typename C>
+__device__ __forceinline__ C fmac_conj(C s, C a, C b) {
+    return fadd(s, fmul_conj(a, b));
+}
+
+// FP32 complex arithmetic on paired single-precision instructions (one instruction
+// does the same operation on both halves of a float2), two per complex multiply:
+//   a b       = (a.x, a.x) * (b.x, b.y) + (-a.y, a.y) * (b.y, b.x)
+//   a conj(b) = (a.x, a.y) * (b.x, b.x) + (a.y, -a.x) * (b.y, b.y)
+// The real and imaginary parts are rounded like the fused scalar forms.
+__device__ __forceinline__ float2 fadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 fmul(float2 a, float2 b) {
+    return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
+}
+__device__ __forceinline__ float2 fmac(float2 s, float2 a, float2 b) {
+    s = __ffma2_rn(make_float2(a.x, a.x), b, s);
+    return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), s);
+}
+__device__ __forceinline__ float2 fmul_conj(float2 a, float2 b) {
+    return __ffma2_rn(make_float2(a.y, -a.x), make_float2(b.y, b.y), __fmul2_rn(a, make_float2(b.x, b.x)));
+}
+__device__ __forceinline__ float2 fmac_conj(float2 s, float2 a, float2 b) {
+    s = __ffma2_rn(a, make_float2(b.x, b.x), s);
+    return __ffma2_rn(make_float2(a.y, -a.x), make_float2(b.y, b.y), s);
+}
 
 __device__ __forceinline__ double frsqrt(double x) { return rsqrt(x); }
 __device__ __forceinline__ float frsqrt(float x) { return rsqrtf(x); }
@@ -180,12 +210,12 @@ __device__ __forceinline__ void fsub_hit(Mt<T> &w, Mt<T> &g) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         C a = w.e[EL(A, c)], b = w.e[EL(B, c)];
-        w.e[EL(A, c)] = fadd(fmul(x00, a), fmul(x01, b));
-        w.e[EL(B, c)] = fadd(fmul(x10, a), fmul(x11, b));
+        w.e[EL(A, c)] = fmac(fmul(x00, a), x01, b);
+        w.e[EL(B, c)] = fmac(fmul(x10, a), x11, b);
         a = g.e[EL(A, c)];
         b = g.e[EL(B, c)];
-        g.e[EL(A, c)] = fadd(fmul(x00, a), fmul(x01, b));
-        g.e[EL(B, c)] = fadd(fmul(x10, a), fmul(x11, b));
+        g.e[EL(A, c)] = fmac(fmul(x00, a), x01, b);
+        g.e[EL(B, c)] = fmac(fmul(x10, a), x11, b);
     }
 }
 
@@ -247,8 +277,8 @@ __device__ __forceinline__ void fprod_left(const Mt<T> &a, const Mt<T> &b, Mt<T>
 #pragma unroll
         for (int j = 0; j < 3; j++) {
             C s = fmul(a.e[EL(i, 0)], b.e[EL(0, j)]);
-            s = fadd(s, fmul(a.e[EL(i, 1)], b.e[EL(1, j)]));
-            s = fadd(s, fmul(a.e[EL(i, 2)], b.e[EL(2, j)]));
+            s = fmac(s, a.e[EL(i, 1)], b.e[EL(1, j)]);
+            s = fmac(s, a.e[EL(i, 2)], b.e[EL(2, j)]);
             c.e[EL(i, j)] = s;
         }
 }
@@ -262,8 +292,8 @@ __device__ __forceinline__ void fprod_dag(const Mt<T> &a, const Mt<T> &b, Mt<T> 
 #pragma unroll
         for (int j = 0; j < 3; j++) {
             C s = fmul_conj(a.e[EL(i, 0)], b.e[EL(j, 0)]);
-            s = fadd(s, fmul_conj(a.e[EL(i, 1)], b.e[EL(j, 1)]));
-            s = fadd(s, fmul_conj(a.e[EL(i, 2)], b.e[EL(j, 2)]));
+            s = fmac_conj(s, a.e[EL(i, 1)], b.e[EL(j, 1)]);
+            s = fmac_conj(s, a.e[EL(i, 2)], b.e[EL(j, 2)]);
             c.e[EL(i, j)] = s;
         }
 }
@@ -320,8 +350,8 @@ __device__ __forceinline__ void apply_forward(typename S::V *__restrict__ p, siz
 #pragma unroll
             for (int j = 0; j < 3; j++) {
                 C s = fmul(up.e[EL(r, 0)], f.e[EL(0, j)]);
-                s = fadd(s, fmul(up.e[EL(r, 1)], f.e[EL(1, j)]));
-                s = fadd(s, fmul(up.e[EL(r, 2)], f.e[EL(2, j)]));
+                s = fmac(s, up.e[EL(r, 1)], f.e[EL(1, j)]);
+                s = fmac(s, up.e[EL(r, 2)], f.e[EL(2, j)]);
                 o[j] = s;
                 if (r < S::STORED_ROWS) p[(size_t)(3 * r + j) * st] = s;
             }
@@ -338,8 +368,8 @@ __device__ __forceinline__ void apply_forward(typename S::V *__restrict__ p, siz
 #pragma unroll
             for (int j = 0; j < 3; j++) {
                 C s = fmul(up.e[EL(r, 0)], f.e[EL(0, j)]);
-                s = fadd(s, fmul(up.e[EL(r, 1)], f.e[EL(1, j)]));
-                s = fadd(s, fmul(up.e[EL(r, 2)], f.e[EL(2, j)]));
+                s = fmac(s, up.e[EL(r, 1)], f.e[EL(1, j)]);
+                s = fmac(s, up.e[EL(r, 2)], f.e[EL(2, j)]);
                 o.e[EL(r, j)] = s;
             }
         S::store(p, st, o);
@@ -373,8 +403,8 @@ __device__ __forceinline__ void apply_backward(typename S::V *__restrict__ p, si
 #pragma unroll
             for (int j = 0; j < 3; j++) {
                 C s = fmul_conj(a0, up.e[EL(j, 0)]);
-                s = fadd(s, fmul_conj(a1, up.e[EL(j, 1)]));
-                s = fadd(s, fmul_conj(a2, up.e[EL(j, 2)]));
+                s = fmac_conj(s, a1, up.e[EL(j, 1)]);
+                s = fmac_conj(s, a2, up.e[EL(j, 2)]);
                 o[j] = s;
                 if (r < S::STORED_ROWS) p[(size_t)(3 * r + j) * st] = s;
             }
@@ -397,8 +427,8 @@ __device__ __forceinline__ void apply_backward(typename S::V *__restrict__ p, si
 #pragma unroll
             for (int j = 0; j < 3; j++) {
                 C s = fmul_conj(m.e[EL(r, 0)], up.e[EL(j, 0)]);
-                s = fadd(s, fmul_conj(m.e[EL(r, 1)], up.e[EL(j, 1)]));
-                s = fadd(s, fmul_conj(m.e[EL(r, 2)], up.e[EL(j, 2)]));
+                s = fmac_conj(s, m.e[EL(r, 1)], up.e[EL(j, 1)]);
+                s = fmac_conj(s, m.e[EL(r, 2)], up.e[EL(j, 2)]);
                 o.e[EL(r, j)] = s;
             }
         }
@@ -506,15 +536,15 @@ __device__ __forceinline__ void apply_staged(const typename S::V *src, int sst, 
                 C v;
                 if (FWD) {
                     v = fmul(up.e[EL(r, 0)], (C)src[j * sst]);
-                    v = fadd(v, fmul(up.e[EL(r, 1)], (C)src[(3 + j) * sst]));
-                    v = fadd(v, fmul(up.e[EL(r, 2)], r2[j]));
+                    v = fmac(v, up.e[EL(r, 1)], (C)src[(3 + j) * sst]);
+                    v = fmac(v, up.e[EL(r, 2)], r2[j]);
                 } else {
                     const C m0 = r < 2 ? (C)src[(3 * r) * sst] : r2[0];
                     const C m1 = r < 2 ? (C)src[(3 * r + 1) * sst] : r2[1];
                     const C m2 = r < 2 ? (C)src[(3 * r + 2) * sst] : r2[2];
                     v = fmul_conj(m0, up.e[EL(j, 0)]);
-                    v = fadd(v, fmul_conj(m1, up.e[EL(j, 1)]));
-                    v = fadd(v, fmul_conj(m2, up.e[EL(j, 2)]));
+                    v = fmac_conj(v, m1, up.e[EL(j, 1)]);
+                    v = fmac_conj(v, m2, up.e[EL(j, 2)]);
                 }
                 o[j] = v;
                 if (r < 2) dst[(size_t)(3 * r + j) * st] = v;
@@ -536,12 +566,12 @@ __device__ __forceinline__ void apply_staged(const typename S::V *src, int sst, 
                 C v;
                 if (FWD) {
                     v = fmul(up.e[EL(r, 0)], m.e[EL(0, j)]);
-                    v = fadd(v, fmul(up.e[EL(r, 1)], m.e[EL(1, j)]));
-                    v = fadd(v, fmul(up.e[EL(r, 2)], m.e[EL(2, j)]));
+                    v = fmac(v, up.e[EL(r, 1)], m.e[EL(1, j)]);
+                    v = fmac(v, up.e[EL(r, 2)], m.e[EL(2, j)]);
                 } else {
                     v = fmul_conj(m.e[EL(r, 0)], up.e[EL(j, 0)]);
-                    v = fadd(v, fmul_conj(m.e[EL(r, 1)], up.e[EL(j, 1)]));
-                    v = fadd(v, fmul_conj(m.e[EL(r, 2)], up.e[EL(j, 2)]));
+                    v = fmac_conj(v, m.e[EL(r, 1)], up.e[EL(j, 1)]);
+                    v = fmac_conj(v, m.e[EL(r, 2)], up.e[EL(j, 2)]);
                 }
                 o.e[EL(r, j)] = v;
             }
