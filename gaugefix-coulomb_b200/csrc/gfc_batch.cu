@@ -37,7 +37,12 @@
 
 namespace gfc {
 
-enum : int { SS_EMPTY = 0, SS_FP32 = 1, SS_PEND = 2, SS_FP64 = 3, SS_DONE = 4 };
+enum : int { SS_EMPTY = 0, SS_FP32 = 1, SS_PEND = 2, SS_FP64 = 3, SS_DONE = 4, SS_VERIFY = 5 };
+// SS_VERIFY: the FP64 e2 measured after half-sweep c - 1 fell below the tolerance, but
+// the timeslice has had half-sweep c too.  Its next pass measures e2 of the state it
+// is in without updating it: below the tolerance -> DONE with that state, else back
+// to FP64 (measured after every half-sweep).  So a retired timeslice's e2 is below
+// the tolerance for the links it keeps, not for an earlier state.
 // e2 of a timeslice after half-sweep c needs the fused sums of its half-sweeps c and
 // c + 1.  While its target (switch threshold or tolerance) is far, a timeslice is
 // measured on own half-sweep counts 30, 31 (mod 32) only; once the last measurement
@@ -87,12 +92,12 @@ __global__ void __launch_bounds__(1024) k_compact(BState b) {
     int c[3] = {0, 0, 0}, act = 0;
     for (int gid = g0; gid < g1; gid++) {
         int st = b.state[gid];
-        b.listed[gid] = st == SS_FP32 || st == SS_FP64;
+        b.listed[gid] = st == SS_FP32 || st == SS_FP64 || st == SS_VERIFY;
         if (st == SS_EMPTY || st == SS_DONE) continue;
         const BSlot &sl = b.slots[gid / b.max_nt];
         act++;
         if (st == SS_FP32) c[0] += sl.nbx;
-        else if (st == SS_FP64) c[1] += sl.nbx;
+        else if (st == SS_FP64 || st == SS_VERIFY) c[1] += sl.nbx;
         else if (st == SS_PEND) c[2] += sl.nfull;
     }
     for (int q = 0; q < 3; q++) sc[q][tid] = c[q];
@@ -115,7 +120,7 @@ __global__ void __launch_bounds__(1024) k_compact(BState b) {
         int st = b.state[gid];
         if (st == SS_EMPTY || st == SS_DONE) continue;
         const BSlot &sl = b.slots[gid / b.max_nt];
-        if (st == SS_FP32 || st == SS_FP64) {
+        if (st == SS_FP32 || st == SS_FP64 || st == SS_VERIFY) {
             int q = st == SS_FP32 ? 0 : 1;
             int2 *lst = q == 0 ? b.items32 : b.items64;
             for (int ch = 0; ch < sl.nbx; ch++, o[q]++)
@@ -186,8 +191,6 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
     __shared__ double sh[2][BCHUNK / 32];
     __shared__ int next[2];
     const int n = b.counts[F64 ? 1 : 0];
-    const int k = b.counts[4];
-    const int par = k & 1;
     const int expect = F64 ? SS_FP64 : SS_FP32;
     const int2 *items = F64 ? b.items64 : b.items32;
     int *cursor = b.counts + (F64 ? 7 : 6);
@@ -209,8 +212,13 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
         const int gid = item.x, chunk = item.y;
         // a timeslice retired earlier in this round still has items in the list;
         // the state is the same for every thread of the CTA
-        if (*(volatile int *)&b.state[gid] == expect) {
-            const int track = b.mflag[gid] & MF_NOW;   // the same for every thread of the CTA
+        const int st = *(volatile int *)&b.state[gid];
+        const bool verify = F64 && st == SS_VERIFY;
+        if (st == expect || verify) {
+            // the same for every thread of the CTA: the parity of the timeslice's own
+            // next half-sweep, and whether this pass measures e2
+            const int par = b.sweeps[gid] & 1;
+            const int track = verify ? 1 : (b.mflag[gid] & MF_NOW);
             const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
             const BSlot &sl = b.slots[slot];
             const Lat l = sl.l;
@@ -219,7 +227,9 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
             const uint32_t vsh = l.vs >> 1;
             const uint32_t off = (uint32_t)chunk * BCHUNK + threadIdx.x;
             double pre = 0.0, post = 0.0;
-            if (off < vsh) {
+            if (off < vsh && verify) {
+                pre = measure_site<S>(u, l, par, (uint32_t)t * vsh + off);
+            } else if (off < vsh) {
                 if constexpr (STG)
                     fast_site_staged<S, BCHUNK, false>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits,
                                                        track, pre, post, (typename S::V *)bstage);
@@ -248,14 +258,13 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
 // threshold, FP64 -> done at the tolerance, NaN -> done with the status bit.
 __global__ void k_bslice(BState b) {
     const int lane = threadIdx.x & 31;
-    const int k = b.counts[4];
     for (int gid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gid < b.nslices;
          gid += (gridDim.x * blockDim.x) >> 5) {
         const int st = b.state[gid];
         // swept in this half-sweep: listed at the round's start and not retired since
         // (a timeslice switched to FP64 at the start of the round has no items yet)
-        if (!b.listed[gid] || (st != SS_FP32 && st != SS_FP64)) continue;   // uniform in the warp
-        const int f = b.mflag[gid];
+        if (!b.listed[gid] || (st != SS_FP32 && st != SS_FP64 && st != SS_VERIFY)) continue;   // uniform in the warp
+        const int f = st == SS_VERIFY ? MF_NOW : b.mflag[gid];
         const int c = b.sweeps[gid];   // this half-sweep's own index
         const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
         const BSlot &sl = b.slots[slot];
@@ -273,11 +282,28 @@ __global__ void k_bslice(BState b) {
             }
         }
         if (lane != 0) continue;
+        if (st == SS_VERIFY) {
+            // measure-only pass: e2 of the current state = post of the last half-sweep
+            // applied (index c - 1) + the other parity now; nothing was applied
+            const double *rlast = b.ring + ((size_t)((c + 1) & 1) * b.nslices + gid) * 2;
+            const double e2s = (s0 + rlast[1]) / (double)sl.l.vs;
+            if (!(s0 == s0)) {
+                atomicOr(b.status, GFC_STATUS_NAN);
+                b.state[gid] = SS_DONE;
+            } else if (e2s <= b.tol) {
+                b.state[gid] = SS_DONE;
+            } else {
+                b.mflag[gid] = MF_NOW | MF_PREV | MF_DENSE;
+                b.state[gid] = SS_FP64;
+            }
+            continue;
+        }
         int nf = f & MF_DENSE;
         int nst = st;
         if (f & MF_NOW) {
-            double *rprev = b.ring + ((size_t)((k + 1) & 1) * b.nslices + gid) * 2;
-            double *rcur = b.ring + ((size_t)(k & 1) * b.nslices + gid) * 2;
+            // ring by the timeslice's own half-sweep index: (pre, post) of c and c - 1
+            double *rprev = b.ring + ((size_t)((c + 1) & 1) * b.nslices + gid) * 2;
+            double *rcur = b.ring + ((size_t)(c & 1) * b.nslices + gid) * 2;
             rcur[0] = s0;
             rcur[1] = s1;
             if (!(s0 == s0) || !(s1 == s1)) {
@@ -287,7 +313,7 @@ __global__ void k_bslice(BState b) {
                 const double e2s = (s0 + rprev[1]) / (double)sl.l.vs;   // e2 after half-sweep c - 1
                 const double target = st == SS_FP32 ? b.switch_e2 : b.tol;
                 if (e2s <= target) {
-                    nst = st == SS_FP32 ? SS_PEND : SS_DONE;
+                    nst = st == SS_FP32 ? SS_PEND : SS_VERIFY;
                 } else if (!(nf & MF_DENSE)) {
                     if (e2s <= 1e3 * target) {
                         nf |= MF_DENSE;

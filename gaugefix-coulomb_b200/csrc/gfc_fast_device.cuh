@@ -441,6 +441,31 @@ __device__ __forceinline__ void apply_backward(typename S::V *__restrict__ p, si
     }
 }
 
+// The e2 density of a site from its current links, without updating anything (the
+// "pre" of fast_site on its own).
+template <class S>
+__device__ __forceinline__ double measure_site(const typename S::V *__restrict__ u, const Lat &l, int par,
+                                               uint32_t i) {
+    using T = typename S::T;
+    using C = typename CT<T>::t;
+    const int op = par ^ 1;
+    Coord c = coord_cb(l, par, i);
+    Mt<T> w;
+#pragma unroll
+    for (int k = 0; k < 9; k++) w.e[k] = mkc<C>(T(0), T(0));
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        Mt<T> f, r;
+        S::load(u + su_idx<S>(l, d, par, i), l.vh, f);
+        S::load(u + su_idx<S>(l, d, op, back_L(l, c, d) >> 1), l.vh, r);
+#pragma unroll
+        for (int x = 0; x < 3; x++)
+#pragma unroll
+            for (int y = 0; y < 3; y++) w.e[EL(x, y)] = fadd(w.e[EL(x, y)], fadd(f.e[EL(x, y)], fconj(r.e[EL(y, x)])));
+    }
+    return e2_from_w(w);
+}
+
 // One site of a checkerboard half-sweep: w(x) from the three forward and three
 // backward spatial links, the over-relaxed SU(3) update, G(x) <- up G(x) and the six
 // links updated in place.  pre / post receive the site's contributions to e2 before
