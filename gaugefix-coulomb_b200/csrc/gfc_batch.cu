@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
             const int track = verify ? 1 : (b.mflag[gid] & MF_NOW);
             const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
             const BSlot &sl = b.slots[slot];
-            const Lat l = sl.l;
+            const Lat &l = sl.l;
             typename S::V *u, *g;
             slot_fields<S>(sl, u, g);
             const uint32_t vsh = l.vs >> 1;
