@@ -160,3 +160,23 @@ def test_staging_gives_a_valid_fix(stage):
     U1 = U.copy()
     orc.apply_gt(U1, G, ns, nt)
     np.testing.assert_allclose(U1, Uf, atol=1e-12)
+
+
+@pytest.mark.parametrize("elem_bytes,swap", [(4, True), (8, True), (4, False)])
+def test_batch_upload_formats_match_single_lattice(elem_bytes, swap):
+    """A slot loads file bytes (FP32 or FP64, big or native endian) exactly as the
+    single-lattice context does: same links after the reunitarisation of activation."""
+    ns, nt = 4, 6
+    U = gfc.synth_config(ns, nt, 97, 0.5)
+    raw = U.astype((">" if swap else "<") + ("f4" if elem_bytes == 4 else "f8"))
+    with gfc.Lattice(ns, nt) as lat:
+        lat.upload_links(raw, elem_bytes, byteswap=swap)
+        lat.reunitarize()
+        U_single = lat.download_links()
+    with gfc.Batch(max_sites=10 ** 4, max_slots=2, max_nt=8) as b:
+        s = b.add(ns, nt)
+        b.upload(s, raw, elem_bytes, swap)
+        b.activate(s, gfc.PREC_FP64_FAST)
+        b.finalize(s)                  # no round ran: the links as loaded (and reunitarised)
+        U_batch = b.download_links(s)
+    np.testing.assert_allclose(U_batch, U_single, atol=1e-14)
