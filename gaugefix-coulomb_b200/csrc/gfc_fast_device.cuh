@@ -582,7 +582,10 @@ __device__ __forceinline__ void apply_staged(const typename S::V *src, int sst, 
         }
     } else {
         Mt<T> m, o;
-        S::load(src, sst, m);
+        if (FWD || track)
+            S::load(src, sst, m);
+        else
+            S::load_rows01(src, sst, m);   // rows 0 and 1 of r . up^dagger need rows 0 and 1 of r only
 #pragma unroll
         for (int r = 0; r < 3; r++) {
             if (r == 2 && !track) break;

@@ -230,7 +230,7 @@ int  gfc_e2_theta_device_noalloc(int ns, int nt, const double *u_dev, void *stre
 /* A batch holds up to max_slots lattices (even ns, nt <= max_nt, max_sites sites in
  * total) on one GPU.  Every timeslice of every lattice is swept independently
  * (timeslices share no link during the sweeps) and retires when its own e2 falls
- * below the tolerance; with GFC_PREC_MIXED it first runs FP32 bulk sweeps until its
+ * below the tolerance (measured on the links it keeps); with GFC_PREC_MIXED it first runs FP32 bulk sweeps until its
  * e2 falls below options.switch_e2 and is then rebuilt in FP64.  One round = K
  * half-sweeps of all active timeslices, replayed as a captured CUDA graph.  Slots
  * can be added, activated, finalised and removed between rounds (continuous
