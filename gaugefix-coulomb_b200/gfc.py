@@ -194,7 +194,7 @@ class PinnedBuffer:
         return self.array.view(dtype)
 
     def close(self):
-        if self.ptr:
+        if getattr(self, "ptr", None):   # None too when __init__ failed
             lib.gfc_host_free(self.ptr)
             self.ptr = None
 
@@ -213,7 +213,7 @@ class Lattice:
         self.h = h
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):   # None too when __init__ failed
             lib.gfc_ctx_destroy(self.h)
             self.h = None
 
@@ -419,7 +419,7 @@ class Batch:
         self.geom = {}
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):   # None too when __init__ failed
             lib.gfc_batch_destroy(self.h)
             self.h = None
 
@@ -579,7 +579,7 @@ class Server:
         self.geom = {}
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):   # None too when __init__ failed
             lib.gfc_server_destroy(self.h)
             self.h = None
 

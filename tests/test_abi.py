@@ -65,3 +65,44 @@ def test_library_is_sm100a():
     embedded architecture list is read from the ELF notes via the build flags)."""
     mk = open(os.path.join(PKG, "Makefile")).read()
     assert "arch=compute_100a,code=sm_100a" in mk
+
+
+def _has_gpu():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def test_no_gpu_fails_loudly():
+    """Without a GPU there is no fallback: creating a context, a batch or a server
+    returns an error code with a message, and the binding raises."""
+    import pytest
+
+    if _has_gpu():
+        pytest.skip("a GPU is present")
+    lib = ctypes.CDLL(gfc.LIB_PATH)
+    h = ctypes.c_void_p()
+    for call in (lambda: lib.gfc_ctx_create(4, 8, 0, 0, ctypes.byref(h)),
+                 lambda: lib.gfc_batch_create(0, ctypes.c_size_t(4096), 2, 8, ctypes.byref(h)),
+                 lambda: lib.gfc_server_create(0, ctypes.c_size_t(4096), ctypes.c_double(0.5), 2, 8,
+                                               ctypes.byref(h))):
+        rc = call()
+        assert rc < 0 and not h.value
+        assert gfc.last_error()
+    with pytest.raises(gfc.GFCError):
+        gfc.Lattice(4, 8)
+    with pytest.raises(gfc.GFCError):
+        gfc.Batch(max_sites=4096, max_slots=2, max_nt=8)
+
+
+def test_bad_arguments_rejected_before_any_device_work():
+    lib = ctypes.CDLL(gfc.LIB_PATH)
+    h = ctypes.c_void_p()
+    assert lib.gfc_ctx_create(4, 8, 0, 0, None) < 0
+    assert lib.gfc_batch_create(0, ctypes.c_size_t(0), 2, 8, ctypes.byref(h)) == -10   # max_sites 0
+    assert lib.gfc_batch_create(0, ctypes.c_size_t(4096), 0, 8, ctypes.byref(h)) == -10  # no slots
+    assert lib.gfc_server_create(0, ctypes.c_size_t(4096), ctypes.c_double(0.5), 0, 8, ctypes.byref(h)) == -10
+    assert lib.gfc_gaugefix_overrelaxation(4, 8, None, None, None, None, None, 0) == -10
