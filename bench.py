@@ -464,7 +464,10 @@ def serve_requests(n, rate, seed=7):
     return [(float(arrivals[i]), sizes[i][0], sizes[i][1], 1000 + i, float(scales[i])) for i in range(n)]
 
 
-def run_serve(a, gfc, precision, n_req, rate):
+SERVE_WORK_SITES = 16 * 1024 * 1024   # smallest-first: sites sweeping together (one 64^3x128 alone)
+
+
+def run_serve(a, gfc, precision, n_req, rate, policy=None):
     """Poisson stream of requests of mixed sizes through the continuous-batching server.
 
     Latency runs from a request's arrival time to the moment its G is in host
@@ -479,6 +482,8 @@ def run_serve(a, gfc, precision, n_req, rate):
         big = max(ns ** 3 * nt for ns, nt in SERVE_SIZES) * 18 * 8
         srv.reserve_host(big, 3)
         srv.autotune(32, 64)
+        policy = gfc.SERVE_SMALLEST_FIRST if policy is None else policy
+        srv.set_policy(policy, SERVE_WORK_SITES)
         pending = list(reqs)
         live = {}
         lat, done_t, upd, e2max, rounds = [], [], 0, 0.0, 0
@@ -512,7 +517,9 @@ def run_serve(a, gfc, precision, n_req, rate):
                     mean_s=float(np.mean(lat)), configs_per_s=n_req / span, seconds=span,
                     site_updates_per_s=upd / span, max_e2=e2max,
                     sizes={f"{ns}^3x{nt}": sum(1 for r in reqs if (r[1], r[2]) == (ns, nt)) for ns, nt in SERVE_SIZES},
-                    precision={gfc.PREC_MIXED: "mixed", gfc.PREC_FP64_FAST: "fp64"}[precision])
+                    precision={gfc.PREC_MIXED: "mixed", gfc.PREC_FP64_FAST: "fp64"}[precision],
+                    policy={gfc.SERVE_ALL: "all admitted requests sweep together",
+                            gfc.SERVE_SMALLEST_FIRST: f"smallest first, {SERVE_WORK_SITES} sites sweeping"}[policy])
     finally:
         srv.close()
 
@@ -598,6 +605,9 @@ def main():
                 out["precision_form"] = run_precision_form(a, gfc)
             elif m == "serve":
                 out["serve_mixed"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate)
+            elif m == "serve_shared":
+                out["serve_mixed_shared"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate,
+                                                      gfc.SERVE_ALL)
             elif m == "serve64":
                 out["serve_fp64"] = run_serve(a, gfc, gfc.PREC_FP64_FAST, a.serve_requests, a.serve_rate)
         if rk.rank == 0:
@@ -618,6 +628,8 @@ def main():
         if a.serve_requests > 0:
             r["extras"]["serve_mixed"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate)
             r["extras"]["serve_fp64"] = run_serve(a, gfc, gfc.PREC_FP64_FAST, a.serve_requests, a.serve_rate)
+            r["extras"]["serve_mixed_shared"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate,
+                                                          gfc.SERVE_ALL)
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):

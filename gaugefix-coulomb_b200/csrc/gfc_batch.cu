@@ -68,6 +68,7 @@ struct BState {
     int *state;           // [nslices], gid = slot * max_nt + t
     int *sweeps;          // [nslices] half-sweeps applied to the timeslice
     int *listed;          // [nslices] 1 if this round's sweep work lists hold the timeslice
+    const int *held;      // [max_slots] 1: the slot is resident but kept out of the rounds
     int *mflag;           // [nslices] e2 measurement: MF_NOW, MF_PREV, MF_DENSE
     int *mk;              // [nslices] own half-sweep count of the last e2 measurement (-1: none)
     double *me2;          // [nslices] that e2
@@ -92,10 +93,12 @@ __global__ void __launch_bounds__(1024) k_compact(BState b) {
     int c[3] = {0, 0, 0}, act = 0;
     for (int gid = g0; gid < g1; gid++) {
         int st = b.state[gid];
-        b.listed[gid] = st == SS_FP32 || st == SS_FP64 || st == SS_VERIFY;
+        const bool held = b.held[gid / b.max_nt];
+        b.listed[gid] = !held && (st == SS_FP32 || st == SS_FP64 || st == SS_VERIFY);
         if (st == SS_EMPTY || st == SS_DONE) continue;
         const BSlot &sl = b.slots[gid / b.max_nt];
         act++;
+        if (held) continue;   // frozen: no items, no switch this round
         if (st == SS_FP32) c[0] += sl.nbx;
         else if (st == SS_FP64 || st == SS_VERIFY) c[1] += sl.nbx;
         else if (st == SS_PEND) c[2] += sl.nfull;
@@ -118,7 +121,7 @@ __global__ void __launch_bounds__(1024) k_compact(BState b) {
     int overflow = 0;
     for (int gid = g0; gid < g1; gid++) {
         int st = b.state[gid];
-        if (st == SS_EMPTY || st == SS_DONE) continue;
+        if (st == SS_EMPTY || st == SS_DONE || b.held[gid / b.max_nt]) continue;
         const BSlot &sl = b.slots[gid / b.max_nt];
         if (st == SS_FP32 || st == SS_FP64 || st == SS_VERIFY) {
             int q = st == SS_FP32 ? 0 : 1;
@@ -491,7 +494,8 @@ struct gfc_batch {
     size_t max_sites = 0, used_sites = 0;
     std::vector<BSlot> hs;          // host copies of the descriptors
     std::vector<void *> mem;        // per-slot allocation
-    std::vector<int> used, ns, nt, activated;
+    std::vector<int> used, ns, nt, activated, hheld;
+    int *held = nullptr;            // device copy of hheld
     BSlot *dslots = nullptr;
     int *state = nullptr, *sweeps = nullptr, *counts = nullptr, *listed = nullptr, *mflag = nullptr, *mk = nullptr;
     double *me2 = nullptr;
@@ -535,6 +539,7 @@ extern "C" int gfc_batch_create(int device, size_t max_sites, int max_slots, int
     b->ns.assign(max_slots, 0);
     b->nt.assign(max_slots, 0);
     b->activated.assign(max_slots, 0);
+    b->hheld.assign(max_slots, 0);
     // work lists: every chunk of every timeslice (upper bound)
     b->cap_items = (int)(max_sites / 2 / BCHUNK + (size_t)b->nslices + 1024);
     b->cap_pend = (int)(max_sites / BCHUNK + (size_t)b->nslices + 1024);
@@ -552,6 +557,8 @@ extern "C" int gfc_batch_create(int device, size_t max_sites, int max_slots, int
     BTRY(cudaMalloc(&b->state, sizeof(int) * b->nslices));
     BTRY(cudaMemset(b->state, 0, sizeof(int) * b->nslices));
     BTRY(cudaMalloc(&b->sweeps, sizeof(int) * b->nslices));
+    BTRY(cudaMalloc(&b->held, sizeof(int) * max_slots));
+    BTRY(cudaMemset(b->held, 0, sizeof(int) * max_slots));
     BTRY(cudaMalloc(&b->listed, sizeof(int) * b->nslices));
     BTRY(cudaMemset(b->listed, 0, sizeof(int) * b->nslices));
     BTRY(cudaMalloc(&b->mflag, sizeof(int) * b->nslices));
@@ -608,6 +615,7 @@ extern "C" int gfc_batch_destroy(gfc_batch *b) {
     cudaFree(b->state);
     cudaFree(b->sweeps);
     cudaFree(b->listed);
+    cudaFree(b->held);
     cudaFree(b->mflag);
     cudaFree(b->mk);
     cudaFree(b->me2);
@@ -702,6 +710,11 @@ extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
     b->mem[slot] = m;
     b->used[slot] = 1;
     b->activated[slot] = 0;
+    if (b->hheld[slot]) {
+        b->hheld[slot] = 0;
+        GFC_CHECK(cudaMemcpyAsync(b->held + slot, &b->hheld[slot], sizeof(int), cudaMemcpyHostToDevice, b->s));
+        GFC_CHECK(cudaStreamSynchronize(b->s));
+    }
     b->ns[slot] = ns;
     b->nt[slot] = nt;
     b->used_sites += V;
@@ -714,6 +727,20 @@ extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
         b->part_n = need;
     }
     *slot_out = slot;
+    return GFC_OK;
+}
+
+// Keep a slot resident but out of the next rounds (hold != 0), or let it sweep again.
+// Its timeslices keep their state, counts and measurements, so holding a lattice for
+// some rounds changes when it finishes, not what it computes.
+extern "C" int gfc_batch_hold(gfc_batch *b, int slot, int hold) {
+    if (!b || slot < 0 || slot >= b->max_slots || !b->used[slot]) return GFC_ERR_ARG;
+    const int v = hold != 0;
+    if (b->hheld[slot] == v) return GFC_OK;
+    GFC_CHECK(cudaSetDevice(b->dev));
+    b->hheld[slot] = v;
+    GFC_CHECK(cudaMemcpyAsync(b->held + slot, &b->hheld[slot], sizeof(int), cudaMemcpyHostToDevice, b->s));
+    GFC_CHECK(cudaStreamSynchronize(b->s));
     return GFC_OK;
 }
 
@@ -819,6 +846,7 @@ static BState make_state(gfc_batch *b, const gfc_params *p, const gfc_options *o
     s.state = b->state;
     s.sweeps = b->sweeps;
     s.listed = b->listed;
+    s.held = b->held;
     s.mflag = b->mflag;
     s.mk = b->mk;
     s.me2 = b->me2;

@@ -11,6 +11,7 @@
 // Lattices therefore join and leave while others are on the GPU, and a lattice's
 // result does not depend on what it shares the GPU with (rounds are aligned and
 // every decision is per timeslice).
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstdlib>
@@ -140,6 +141,9 @@ struct gfc_server {
     std::deque<int64_t> queue;        // main thread
     std::map<int, int64_t> slot_req;  // main thread: slots in use (sweeping or copying out)
     int runnable = 0;                 // main thread: slots still sweeping
+    int policy = GFC_SERVE_ALL;       // main thread: which admitted requests sweep each round
+    size_t work_sites = 0;            //   GFC_SERVE_SMALLEST_FIRST: sites swept together
+    std::map<int, int> held;          // main thread: slot -> held by the policy
     // shared with the result thread (under mu)
     std::mutex mu;
     std::condition_variable cv;
@@ -288,6 +292,7 @@ extern "C" int gfc_server_step(gfc_server *s, const gfc_params *p, const gfc_opt
         int rc = gfc_batch_remove(s->b, slot);
         if (rc) return rc;
         s->slot_req.erase(slot);
+        s->held.erase(slot);
     }
     double t1 = now_s();
     s->sec[0] += t1 - t0;
@@ -319,6 +324,34 @@ extern "C" int gfc_server_step(gfc_server *s, const gfc_params *p, const gfc_opt
         s->slot_req[slot] = r->id;
         s->runnable++;
         it = s->queue.erase(it);
+    }
+    // which admitted requests sweep in this round
+    if (s->policy == GFC_SERVE_SMALLEST_FIRST) {
+        std::vector<std::pair<size_t, int64_t>> run;   // (sites, id) of requests still sweeping
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            for (auto &kv : s->slot_req) {
+                const Request &r = s->req[kv.second];
+                if (r.state == REQ_RUNNING && r.slot >= 0)
+                    run.push_back({(size_t)r.ns * r.ns * r.ns * r.nt, r.id});
+            }
+        }
+        std::sort(run.begin(), run.end());
+        size_t cum = 0;
+        for (auto &e : run) {
+            int slot;
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                slot = s->req[e.second].slot;
+            }
+            const int hold = cum > 0 && cum + e.first > s->work_sites;
+            if (!hold) cum += e.first;
+            if (s->held[slot] != hold) {
+                int rc = gfc_batch_hold(s->b, slot, hold);
+                if (rc) return rc;
+                s->held[slot] = hold;
+            }
+        }
     }
     double t2 = now_s();
     s->sec[1] += t2 - t1;
@@ -430,6 +463,24 @@ extern "C" int gfc_server_reserve_host(gfc_server *s, size_t buffer_bytes, int c
     std::lock_guard<std::mutex> lk(s->mu);
     for (void *p : got) s->host.give(p);
     return (int)got.size() == count ? GFC_OK : GFC_ERR_NOMEM;
+}
+
+// Scheduling of admitted requests.  GFC_SERVE_ALL: every admitted request sweeps in
+// every round (they share the GPU).  GFC_SERVE_SMALLEST_FIRST: the requests still
+// sweeping are taken smallest first until work_sites sites are sweeping (at least
+// one); the others stay resident and wait.  Admission is by free memory either way.
+extern "C" int gfc_server_set_policy(gfc_server *s, int policy, size_t work_sites) {
+    if (!s || (policy != GFC_SERVE_ALL && policy != GFC_SERVE_SMALLEST_FIRST)) return GFC_ERR_ARG;
+    if (policy == GFC_SERVE_ALL)
+        for (auto &kv : s->held)
+            if (kv.second) {
+                int rc = gfc_batch_hold(s->b, kv.first, 0);
+                if (rc) return rc;
+                kv.second = 0;
+            }
+    s->policy = policy;
+    s->work_sites = work_sites;
+    return GFC_OK;
 }
 
 // Host seconds spent in the four phases of gfc_server_step (release, admission,

@@ -395,6 +395,7 @@ def _bind_batch():
         "gfc_batch_stream": (P, [P]),
         "gfc_batch_set_shape": (I, [P, I, I, I]),
         "gfc_batch_set_staging": (I, [P, I]),
+        "gfc_batch_hold": (I, [P, I, I]),
         "gfc_batch_get_shape": (I, [P] + [IP] * 4),
         "gfc_batch_autotune": (I, [P, I, I, ctypes.POINTER(D)]),
         "gfc_batch_fix_all": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), RP]),
@@ -505,6 +506,9 @@ class Batch:
     def set_shape(self, minb32=4, minb64=3, round_sweeps=8):
         _check(lib.gfc_batch_set_shape(self.h, minb32, minb64, round_sweeps), "set_shape")
 
+    def hold(self, slot, hold=True):
+        _check(lib.gfc_batch_hold(self.h, slot, int(hold)), "gfc_batch_hold")
+
     def set_staging(self, stage64):
         _check(lib.gfc_batch_set_staging(self.h, int(stage64)), "set_staging")
 
@@ -551,6 +555,7 @@ def _bind_server():
                                   ctypes.POINTER(ctypes.c_size_t)]),
         "gfc_server_batch": (P, [P]),
         "gfc_server_reserve_host": (I, [P, S, I]),
+        "gfc_server_set_policy": (I, [P, I, S]),
         "gfc_server_stats": (I, [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]),
     }
     for name, (res, args) in sig.items():
@@ -562,6 +567,7 @@ def _bind_server():
 _bind_server()
 
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FETCHED = 0, 1, 2, 3
+SERVE_ALL, SERVE_SMALLEST_FIRST = 0, 1
 
 
 class Server:
@@ -638,6 +644,11 @@ class Server:
         a = np.ctypeslib.as_array(p, shape=(n.value,))
         a.flags.writeable = False
         return a
+
+    def set_policy(self, policy, work_sites=0):
+        """SERVE_ALL: every admitted request sweeps each round; SERVE_SMALLEST_FIRST:
+        the smallest running requests, up to work_sites sites, the others wait."""
+        _check(lib.gfc_server_set_policy(self.h, policy, int(work_sites)), "gfc_server_set_policy")
 
     def reserve_host(self, buffer_bytes, count):
         """Pin host result buffers ahead of time."""

@@ -241,6 +241,9 @@ int    gfc_batch_destroy(gfc_batch *b);
 size_t gfc_batch_slot_bytes(int ns, int nt);          /* device bytes one slot needs */
 int    gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot);   /* GFC_ERR_BUSY when full */
 int    gfc_batch_remove(gfc_batch *b, int slot);
+/* hold != 0: keep the slot resident but out of the rounds (its state is kept, so
+ * holding changes when it finishes, not what it computes); 0: sweep it again */
+int    gfc_batch_hold(gfc_batch *b, int slot, int hold);
 /* links in (raw reference-layout bytes, as gfc_ctx_upload_links), reunitarised */
 int    gfc_batch_upload(gfc_batch *b, int slot, const void *host, int elem_bytes, int byteswap);
 /* the seeded synthetic configuration of gfc_synth_config built on the device
@@ -306,6 +309,13 @@ int    gfc_server_fetch(gfc_server *s, int64_t id, void *gt, int elem_bytes, int
 /* pin `count` host buffers of `buffer_bytes` for results ahead of time (results
  * go to reused page-locked buffers, up to 32 GiB of them) */
 int    gfc_server_reserve_host(gfc_server *s, size_t buffer_bytes, int count);
+/* Scheduling of admitted requests (admission itself is by free memory either way):
+ * GFC_SERVE_ALL (default) sweeps every admitted request in every round;
+ * GFC_SERVE_SMALLEST_FIRST sweeps the requests still running smallest first, as many
+ * as fit in work_sites sites (at least one), the others wait resident. */
+#define GFC_SERVE_ALL            0
+#define GFC_SERVE_SMALLEST_FIRST 1
+int    gfc_server_set_policy(gfc_server *s, int policy, size_t work_sites);
 /* host seconds in the phases of gfc_server_step (release, admission, rounds,
  * finalisation) and the rounds run */
 int    gfc_server_stats(const gfc_server *s, double *seconds4, long long *rounds);

@@ -180,3 +180,34 @@ def test_batch_upload_formats_match_single_lattice(elem_bytes, swap):
         b.finalize(s)                  # no round ran: the links as loaded (and reunitarised)
         U_batch = b.download_links(s)
     np.testing.assert_allclose(U_batch, U_single, atol=1e-14)
+
+
+def test_held_slot_gives_the_same_result():
+    """A slot kept out of some rounds (resident, frozen) ends with the G it gets alone."""
+    ns, nt = 6, 6
+    U = gfc.synth_config(ns, nt, 98, 0.6)
+    p, o = params(), gfc.options(precision=gfc.PREC_MIXED)
+    with gfc.Batch(max_sites=10 ** 5, max_slots=2, max_nt=8) as b:
+        s = b.add(ns, nt)
+        b.upload(s, U, 8, False)
+        b.activate(s, gfc.PREC_MIXED)
+        b.fix_all(p, o)
+        G_alone = b.download_gt(s)
+    with gfc.Batch(max_sites=10 ** 5, max_slots=4, max_nt=8) as b:
+        other = b.add(4, 8)
+        b.upload(other, gfc.synth_config(4, 8, 99, 0.5), 8, False)
+        b.activate(other, gfc.PREC_MIXED)
+        s = b.add(ns, nt)
+        b.upload(s, U, 8, False)
+        b.activate(s, gfc.PREC_MIXED)
+        for r in range(12):                      # hold it now and then, in FP32 and FP64 phases
+            b.hold(s, r % 3 == 1 or 5 <= r <= 7)
+            b.round(p, o)
+        b.hold(s, False)
+        active, rounds = 1, 0
+        while active and rounds < 1000:
+            active = b.round(p, o)
+            rounds += 1
+        assert active == 0
+        b.finalize(s)
+        assert b.download_gt(s).tobytes() == G_alone.tobytes()

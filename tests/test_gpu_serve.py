@@ -68,3 +68,19 @@ def test_uploaded_and_synthetic_requests_mix():
         out = run_until_done(srv, [a, b], p, o)
     assert out[a].tobytes() == alone(6, 6, 0, 0, gfc.PREC_FP64_FAST, links=U).tobytes()
     assert out[b].tobytes() == alone(4, 10, 112, 0.5, gfc.PREC_FP64_FAST).tobytes()
+
+
+def test_smallest_first_policy():
+    """With one request sweeping at a time, smallest first: the small request that
+    arrived second finishes first; both results are those of the lattice alone."""
+    p = gfc.default_params(tolerance=TOL)
+    o = gfc.options(precision=gfc.PREC_MIXED)
+    with gfc.Server(max_sites=10 ** 5, max_slots=4, max_nt=16) as srv:
+        srv.set_policy(gfc.SERVE_SMALLEST_FIRST, 1)
+        big = srv.submit(8, 8, seed=121, scale=0.5)
+        small = srv.submit(4, 4, seed=122, scale=0.5)
+        out = run_until_done(srv, [big, small], p, o)
+        t_big, t_small = srv.poll(big)[2], srv.poll(small)[2]
+    assert t_small < t_big
+    assert out[big].tobytes() == alone(8, 8, 121, 0.5, gfc.PREC_MIXED).tobytes()
+    assert out[small].tobytes() == alone(4, 4, 122, 0.5, gfc.PREC_MIXED).tobytes()
