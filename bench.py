@@ -400,11 +400,16 @@ def parse_mix(spec):
     return mix
 
 
-def run_batch(a, gfc, torch, precision):
+def run_batch(a, gfc, torch, precision, rk=None):
     """The 96-config mix (32 each of 16^3x32, 24^3x48, 32^3x64) in one batch: every
-    timeslice retires on its own e2."""
-    mix = parse_mix(a.batch_mix)
-    scales = batch_scales(len(mix))
+    timeslice retires on its own e2.  Under torchrun the configs are dealt to the
+    ranks (config k to rank k mod N, one batch per GPU, no exchange); the time is the
+    slowest rank's."""
+    mix_all = parse_mix(a.batch_mix)
+    scales = batch_scales(len(mix_all))
+    world, rank = (rk.world, rk.rank) if rk else (1, 0)
+    mine = list(range(rank, len(mix_all), world))
+    mix = [mix_all[k] for k in mine]
     sites = sum(ns ** 3 * nt for ns, nt in mix)
     big = max(set(mix), key=lambda g: g[0] ** 3 * g[1])
     b = gfc.Batch(max_sites=sites + big[0] ** 3 * big[1], max_slots=len(mix) + 1,
@@ -417,7 +422,7 @@ def run_batch(a, gfc, torch, precision):
         stream = torch.cuda.ExternalStream(b.stream)
         slots = []
         t0 = time.perf_counter()
-        for k, (ns, nt) in enumerate(mix):
+        for k, (ns, nt) in zip(mine, mix):
             s = b.add(ns, nt)
             b.synth(s, 100 + k, float(scales[k]))
             slots.append(s)
@@ -428,6 +433,9 @@ def run_batch(a, gfc, torch, precision):
         params = gfc.default_params(tolerance=a.tol)
         opts = gfc.options(precision=precision)
         l0 = b.kernel_launches
+        if rk:
+            rk.barrier()
+        torch.cuda.synchronize()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         t0 = time.perf_counter()
@@ -437,6 +445,9 @@ def run_batch(a, gfc, torch, precision):
         wall = time.perf_counter() - t0
         dev = ev0.elapsed_time(ev1) * 1e-3
         upd = sum(site_updates(b, s, ns, nt) for s, (ns, nt) in zip(slots, mix))
+        if rk:
+            dev, upd, _ = rk.aggregate(dev, upd)
+            wall = rk.reduce(wall, "MAX")
         per_size = {}
         for s, (ns, nt) in zip(slots, mix):
             sw = b.slice_sweeps(s)
@@ -447,9 +458,10 @@ def run_batch(a, gfc, torch, precision):
             d["slice_sweeps_min"] = min(d["slice_sweeps_min"], int(sw.min()))
             d["slice_sweeps_max"] = max(d["slice_sweeps_max"], int(sw.max()))
             d["not_converged"] += int(reps[s].status <= 0)
-        return dict(configs=len(mix), sites=sites, seconds=dev, seconds_wall=wall, setup_seconds=t_setup,
+        return dict(configs=len(mix_all), ranks=world, sites=rk.reduce(sites, "SUM") if rk else sites,
+                    seconds=dev, seconds_wall=wall, setup_seconds=t_setup,
                     autotune_seconds=t_tune, autotune=tune, shape=b.shape(),
-                    rounds=rounds, site_updates=upd, site_updates_per_s=upd / dev, configs_per_s=len(mix) / dev,
+                    rounds=rounds, site_updates=upd, site_updates_per_s=upd / dev, configs_per_s=len(mix_all) / dev,
                     kernel_launches=b.kernel_launches - l0, status=b.status(), per_size=per_size,
                     precision={gfc.PREC_MIXED: "mixed", gfc.PREC_FP64_FAST: "fp64"}[precision])
     finally:
@@ -598,9 +610,9 @@ def main():
         out = {}
         for m in a.only.split(","):
             if m == "batch":
-                out["batch_mixed"] = run_batch(a, gfc, torch, gfc.PREC_MIXED)
+                out["batch_mixed"] = run_batch(a, gfc, torch, gfc.PREC_MIXED, rk)
             elif m == "batch64":
-                out["batch_fp64"] = run_batch(a, gfc, torch, gfc.PREC_FP64_FAST)
+                out["batch_fp64"] = run_batch(a, gfc, torch, gfc.PREC_FP64_FAST, rk)
             elif m == "precision":
                 out["precision_form"] = run_precision_form(a, gfc)
             elif m == "serve":
@@ -616,15 +628,15 @@ def main():
         return
 
     r = run_gfc(a, rk)
+    import torch
+
+    import gfc
+
+    if not a.no_batch:   # on every rank: the configs are dealt to the GPUs
+        r["extras"]["batch_mixed"] = run_batch(a, gfc, torch, gfc.PREC_MIXED, rk)
     if rk.world == 1:
-        import torch
-
-        import gfc
-
         if not a.no_precision_form and not a.no_extras:
             r["extras"]["precision_form"] = run_precision_form(a, gfc)
-        if not a.no_batch:
-            r["extras"]["batch_mixed"] = run_batch(a, gfc, torch, gfc.PREC_MIXED)
         if a.serve_requests > 0:
             r["extras"]["serve_mixed"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate)
             r["extras"]["serve_fp64"] = run_serve(a, gfc, gfc.PREC_FP64_FAST, a.serve_requests, a.serve_rate)
