@@ -106,3 +106,14 @@ def test_bad_arguments_rejected_before_any_device_work():
     assert lib.gfc_batch_create(0, ctypes.c_size_t(4096), 0, 8, ctypes.byref(h)) == -10  # no slots
     assert lib.gfc_server_create(0, ctypes.c_size_t(4096), ctypes.c_double(0.5), 0, 8, ctypes.byref(h)) == -10
     assert lib.gfc_gaugefix_overrelaxation(4, 8, None, None, None, None, None, 0) == -10
+
+
+def test_geometry_limits_rejected_before_any_device_work():
+    """Extents the 32-bit site indexing cannot address, and empty extents, are refused
+    with GFC_ERR_GEOMETRY before anything touches a device."""
+    lib = ctypes.CDLL(gfc.LIB_PATH)
+    h = ctypes.c_void_p()
+    assert lib.gfc_ctx_create(512, 512, 0, 0, ctypes.byref(h)) == -13   # 4V > 2^31
+    assert lib.gfc_ctx_create(0, 8, 0, 0, ctypes.byref(h)) == -13
+    assert lib.gfc_ctx_create(4, -1, 0, 0, ctypes.byref(h)) == -13
+    assert "too large" in gfc.last_error() or "extents" in gfc.last_error()
