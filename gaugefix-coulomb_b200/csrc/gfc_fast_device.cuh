@@ -251,8 +251,14 @@ template <typename T>
 __device__ __forceinline__ void fupdate(Mt<T> &w, T omega, unsigned hits, Mt<T> &g) {
     using C = typename CT<T>::t;
     fidentity(g);
+    if (hits > 0) {   // the first hit written out: g is still the identity, so the
+                      // compiler drops the products with its zeros and ones
+        fsub_hit<0, 1>(w, g);
+        fsub_hit<0, 2>(w, g);
+        fsub_hit<1, 2>(w, g);
+    }
 #pragma unroll 1
-    for (unsigned h = 0; h < hits; h++) {
+    for (unsigned h = 1; h < hits; h++) {
         fsub_hit<0, 1>(w, g);
         fsub_hit<0, 2>(w, g);
         fsub_hit<1, 2>(w, g);
