@@ -476,7 +476,7 @@ def serve_requests(n, rate, seed=7):
     return [(float(arrivals[i]), sizes[i][0], sizes[i][1], 1000 + i, float(scales[i])) for i in range(n)]
 
 
-SERVE_WORK_SITES = 16 * 1024 * 1024   # smallest-first: sites sweeping together (one 64^3x128 alone)
+SERVE_WORK_SITES = 40 * 1024 * 1024   # smallest-first: sites sweeping together (one 64^3x128 and others)
 
 
 def run_serve(a, gfc, precision, n_req, rate, policy=None):
