@@ -483,6 +483,17 @@ extern "C" int gfc_ctx_halfsweeps(gfc_ctx *c, int first_sweep, int n, float omeg
     return GFC_OK;
 }
 
+// applyGaugeTransformationU (fields.c:375-435) with the resident G on all links.
+extern "C" int gfc_ctx_apply_gt(gfc_ctx *c) {
+    if (!c) return GFC_ERR_ARG;
+    if (!c->has_links) return GFC_ERR_STATE;
+    GFC_CHECK(cudaSetDevice(c->dev));
+    launch_apply_gt(c->u, c->ut, c->g, c->lat, 1, c->s);
+    c->launches++;
+    GFC_CHECK(cudaGetLastError());
+    return GFC_OK;
+}
+
 extern "C" int gfc_ctx_finalize_temporal(gfc_ctx *c) {
     if (!c) return GFC_ERR_ARG;
     GFC_CHECK(cudaSetDevice(c->dev));
@@ -634,9 +645,22 @@ extern "C" int gfc_ctx_fix(gfc_ctx *c, const gfc_params *p, const gfc_options *o
     }
     GFC_CHECK(cudaSetDevice(c->dev));
     long long l0 = c->launches;
+    if (opt->warm_start && opt->precision == GFC_PREC_MIXED) {
+        set_error("a warm start runs on the FP64 paths (not GFC_PREC_MIXED)");
+        r->status = GFC_ERR_ARG;
+        return GFC_ERR_ARG;
+    }
     GFC_CHECK(cudaEventRecord(c->ev_a, c->s));
-    launch_identity(c->g, c->lat, c->s);
-    c->launches += c->lat.npar;
+    if (opt->warm_start) {
+        // the resident G is the starting transformation: fix G0 U G0^dagger (spatial
+        // links now, temporal ones with the final G at the end) and keep accumulating
+        // into G0, so the returned G is the whole transformation of the uploaded links
+        launch_apply_gt(c->u, c->ut, c->g, c->lat, 0, c->s);
+        c->launches++;
+    } else {
+        launch_identity(c->g, c->lat, c->s);
+        c->launches += c->lat.npar;
+    }
 
     int ret;
     if (opt->precision == GFC_PREC_MIXED && c->lat.cb) {

@@ -42,6 +42,8 @@ void launch_store_links(const double2 *u, const double2 *ut, const Lat &l, uint3
 void launch_temporal_transform(double2 *ut, const double2 *g, const Lat &l, cudaStream_t s);
 // u_d(x) <- G(x) u0_d(x) G(x+d)^dagger for the spatial links (rebuild from originals)
 void launch_apply_gt_spatial(double2 *u, const double2 *u0, const double2 *g, const Lat &l, cudaStream_t s);
+// applyGaugeTransformationU in the reference's arithmetic, in place (temporal: also ut)
+void launch_apply_gt(double2 *u, double2 *ut, const double2 *g, const Lat &l, int temporal, cudaStream_t s);
 // format conversions over nblk SoA blocks of `stride` matrices (gfc_fast.cu)
 void launch_to_f32(const double2 *src, float4 *dst, uint32_t stride, uint32_t nblk, cudaStream_t s);
 void launch_identity32(float4 *g, uint32_t stride, uint32_t nblk, cudaStream_t s);

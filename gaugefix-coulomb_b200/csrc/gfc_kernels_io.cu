@@ -180,6 +180,55 @@ __global__ void k_apply_gt_spatial(double2 *__restrict__ u, const double2 *__res
     }
 }
 
+// prod_vuwdagger3x3 (SU3_ops.c:688-730) in its own order: o_ab = sum_c sum_d
+// (v_ac u_cd) conj(w_bd), accumulated from zero, every product and sum rounded alone
+__device__ __forceinline__ void xvuwdag(const M3 &v, const M3 &u, const M3 &w, M3 &o) {
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            double2 s = cz();
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int d = 0; d < 3; d++)
+                    s = xcadd(s, xcmul(xcmul(v.e[EL(a, c)], u.e[EL(c, d)]), cconj(w.e[EL(b, d)])));
+            o.e[EL(a, b)] = s;
+        }
+}
+
+// applyGaugeTransformationU (fields.c:375-435), in place: U_mu(x) <- G(x) U_mu(x)
+// G(x+mu)^dagger for the spatial links and, with temporal != 0, the temporal ones.
+// Each thread reads and writes only the links of its own site.
+__global__ void k_apply_gt(double2 *__restrict__ u, double2 *__restrict__ ut, const double2 *__restrict__ g,
+                           Lat l, int temporal) {
+    uint32_t L = blockIdx.x * blockDim.x + threadIdx.x;
+    if (L >= l.v) return;
+    Coord c = coord_lex(l, L);
+    Slot s = slot_of(l, L);
+    M3 gx, gy, uu, o;
+    load_m(g + gidx(l, s.par, 0, s.i), l.vh, gx);
+    if (temporal) {
+        Slot sy = slot_of(l, fwd_t_L(l, c));
+        load_m(g + gidx(l, sy.par, 0, sy.i), l.vh, gy);
+        load_m(ut + gidx(l, s.par, 0, s.i), l.vh, uu);
+        xvuwdag(gx, uu, gy, o);
+        store_m(ut + gidx(l, s.par, 0, s.i), l.vh, o);
+    }
+#pragma unroll 1
+    for (int d = 0; d < 3; d++) {
+        Slot sy = slot_of(l, fwd_L(l, c, d));
+        load_m(g + gidx(l, sy.par, 0, sy.i), l.vh, gy);
+        load_m(u + uidx(l, d, s.par, 0, s.i), l.vh, uu);
+        xvuwdag(gx, uu, gy, o);
+        store_m(u + uidx(l, d, s.par, 0, s.i), l.vh, o);
+    }
+}
+
+void launch_apply_gt(double2 *u, double2 *ut, const double2 *g, const Lat &l, int temporal, cudaStream_t s) {
+    k_apply_gt<<<(l.v + 127) / 128, 128, 0, s>>>(u, ut, g, l, temporal);
+}
+
 void launch_apply_gt_spatial(double2 *u, const double2 *u0, const double2 *g, const Lat &l, cudaStream_t s) {
     k_apply_gt_spatial<<<(l.v + 127) / 128, 128, 0, s>>>(u, u0, g, l);
 }

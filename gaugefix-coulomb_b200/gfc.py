@@ -52,6 +52,7 @@ class Options(ctypes.Structure):
         ("refine_reunit", ctypes.c_uint),
         ("block_threads", ctypes.c_int),
         ("dense_check", ctypes.c_int),
+        ("warm_start", ctypes.c_int),
     ]
 
 
@@ -122,6 +123,7 @@ def _load():
         "gfc_ctx_halfsweeps": (I, [P, I, I, ctypes.c_float, U, I]),
         "gfc_ctx_finalize_temporal": (I, [P]),
         "gfc_ctx_fix": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), ctypes.POINTER(Report)]),
+        "gfc_ctx_apply_gt": (I, [P]),
         "gfc_gaugefix_overrelaxation": (I, [I, I, P, P, ctypes.POINTER(Params), ctypes.POINTER(Options),
                                             ctypes.POINTER(Report), I]),
         "gfc_e2_theta_device_noalloc": (I, [I, I, P, P, DP, DP]),
@@ -277,6 +279,10 @@ class Lattice:
 
     def halfsweeps(self, first, n, omega=1.95, hits=2, precision=PREC_FP64_EXACT):
         _check(lib.gfc_ctx_halfsweeps(self.h, first, n, omega, hits, precision), "halfsweeps")
+
+    def apply_gt(self):
+        """applyGaugeTransformationU with the resident G on all links."""
+        _check(lib.gfc_ctx_apply_gt(self.h), "apply_gt")
 
     def finalize_temporal(self):
         _check(lib.gfc_ctx_finalize_temporal(self.h), "finalize_temporal")

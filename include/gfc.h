@@ -93,6 +93,11 @@ typedef struct {
                                  on one pair of half-sweeps per 32 while the measured rate
                                  says the tolerance is far, then after every half-sweep;
                                  1 measures after every half-sweep throughout            */
+    int    warm_start;        /* 1: the resident G (gfc_ctx_upload_gt) is the starting
+                                 transformation: the fix works on G U G^dagger and the G
+                                 it returns includes it (loadGaugeTransf +
+                                 applyGaugeTransformationU, fields_io.c:309-402,
+                                 fields.c:375-435, then the fix); FP64 paths only      */
 } gfc_options;
 
 void gfc_options_default(gfc_options *o);
@@ -186,6 +191,9 @@ int  gfc_ctx_plaquette(gfc_ctx *c, double *spatial, double *temporal);
 int  gfc_ctx_halfsweeps(gfc_ctx *c, int first_sweep, int n, float omega_OR, unsigned hits, int precision);
 /* apply G to the temporal links (U_t(x) <- G(x) U_t(x) G(x+t)^dagger) and reunitarise them */
 int  gfc_ctx_finalize_temporal(gfc_ctx *c);
+/* applyGaugeTransformationU (fields.c:375-435) with the resident G, on all links, in
+ * the reference's arithmetic */
+int  gfc_ctx_apply_gt(gfc_ctx *c);
 
 /* ---- launch-shape autotuner (no counterpart in the reference) ------------------------ */
 /* Times every compiled launch shape (threads per block x resident blocks per SM)

@@ -86,3 +86,76 @@ def test_projection_failure_reported():
         lat.reunitarize()
         assert lat.status() & 1
         assert lat.status() == 0     # cleared by the read
+
+
+def _mats(G):
+    M = G.reshape(-1, 9, 2)
+    return (M[..., 0] + 1j * M[..., 1]).reshape(-1, 3, 3)
+
+
+def _a_transformation(ns, nt, seed):
+    """An SU(3) field: G after a few half-sweeps of an unconverged fix."""
+    U = gfc.synth_config(ns, nt, seed, 0.5)
+    with gfc.Lattice(ns, nt) as lat:
+        lat.upload_links(U, 8, False)
+        rc, _ = lat.fix(gfc.default_params(max_sweeps_to_fix=7))
+        assert rc == gfc.FIX_NOT_CONVERGED
+        return lat.download_gt()
+
+
+def test_apply_gt_matches_oracle_bitwise():
+    ns, nt = 4, 6
+    U = gfc.synth_config(ns, nt, 131, 0.5)
+    orc.reunitarize(U)
+    G = _a_transformation(ns, nt, 132)
+    with gfc.Lattice(ns, nt) as lat:
+        lat.upload_links(U, 8, False)
+        lat.upload_gt(G, 8, False)
+        lat.apply_gt()
+        Ug = lat.download_links()
+    Uo = U.copy()
+    orc.apply_gt(Uo, G, ns, nt)
+    assert orc.sha(Ug) == orc.sha(Uo)
+
+
+@pytest.mark.parametrize("precision,stop", [(gfc.PREC_FP64_EXACT, gfc.STOP_REFERENCE),
+                                            (gfc.PREC_FP64_FAST, gfc.STOP_EVERY)])
+def test_warm_start(precision, stop):
+    """Fixing from a saved transformation G0: the links fixed are G0 U G0^dagger and
+    the G returned is the whole transformation (the oracle: applyGaugeTransformationU,
+    then the fix, then the product)."""
+    ns, nt = 4, 8
+    U0 = gfc.synth_config(ns, nt, 133, 0.5)
+    orc.reunitarize(U0)
+    G0 = _a_transformation(ns, nt, 134)
+    U1 = U0.copy()
+    orc.apply_gt(U1, G0, ns, nt)
+    Gf = np.zeros_like(G0)
+    rc_o = orc.fix(U1, Gf, ns, nt, tol=1e-15)[0]
+    with gfc.Lattice(ns, nt) as lat:
+        lat.upload_links(U0, 8, False)
+        lat.upload_gt(G0, 8, False)
+        rc, rep = lat.fix(gfc.default_params(tolerance=1e-15),
+                          gfc.options(precision=precision, stop_rule=stop, warm_start=1))
+        G = lat.download_gt()
+        U = lat.download_links()
+    assert rep.final_residue <= 1e-15
+    # the fast path stops at the first half-sweep below the tolerance (the oracle on
+    # the reference schedule later), so its G agrees to what e2 ~ 1e-15 pins down
+    atol = 1e-12 if precision == gfc.PREC_FP64_EXACT else 1e-6
+    np.testing.assert_allclose(_mats(G), _mats(Gf) @ _mats(G0), atol=atol)
+    assert rep.functional == pytest.approx(orc.functional(U1, ns, nt), rel=1e-12)
+    U2 = U0.copy()
+    orc.apply_gt(U2, G, ns, nt)
+    np.testing.assert_allclose(U, U2, atol=1e-12)
+    if precision == gfc.PREC_FP64_EXACT:
+        # the links evolve as in the reference from G0 U G0^dagger, bit for bit
+        assert rc == rc_o
+        assert orc.sha(U.reshape(-1, 4, 18)[:, 1:4, :]) == orc.sha(U1.reshape(-1, 4, 18)[:, 1:4, :])
+
+
+def test_warm_start_refused_on_the_mixed_path():
+    with gfc.Lattice(4, 4, mixed=True) as lat:
+        lat.upload_links(gfc.synth_config(4, 4, 135, 0.5), 8, False)
+        with pytest.raises(gfc.GFCError):
+            lat.fix(gfc.default_params(), gfc.options(precision=gfc.PREC_MIXED, warm_start=1))
