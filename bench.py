@@ -233,9 +233,8 @@ def run_gfc(a, rk):
     lat2.set_shapes(*lat.shapes())
     ctxs = (lat, lat2)
 
-    def issue(ctx):
-        ctx.upload_links(raw.array, 8, byteswap=True)
-        ctx.reunitarize()
+    def issue(ctx):   # byte swap, layout and reunitarisation in one pass on the GPU
+        ctx.upload_links_reunit(raw.array, 8, byteswap=True)
 
     def e2e_run(n):
         lat.sync()

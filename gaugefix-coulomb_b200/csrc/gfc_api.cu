@@ -269,6 +269,20 @@ extern "C" int gfc_ctx_upload_links(gfc_ctx *c, const void *host, int elem_bytes
     return rc;
 }
 
+// loadConfig + reunitarizeField (gauge_fix_coulomb.c:123-131) in one pass: the
+// same links, bit for bit, as gfc_ctx_upload_links followed by gfc_ctx_reunitarize.
+extern "C" int gfc_ctx_upload_links_reunit(gfc_ctx *c, const void *host, int elem_bytes, int byteswap) {
+    if (!c || !host || (elem_bytes != 8 && elem_bytes != 4)) return GFC_ERR_ARG;
+    GFC_CHECK(cudaSetDevice(c->dev));
+    const Lat l = c->lat;
+    size_t per_slice = (size_t)l.vs * 4 * 18 * elem_bytes;
+    int rc = upload_chunked(c, host, per_slice, [&](void *d, uint32_t t0, uint32_t nts) {
+        launch_load_links(d, elem_bytes, byteswap, l, t0, nts, c->u, c->ut, c->s, 1, c->dstatus);
+    });
+    if (rc == GFC_OK) c->has_links = 1;
+    return rc;
+}
+
 extern "C" int gfc_ctx_upload_gt(gfc_ctx *c, const void *host, int elem_bytes, int byteswap) {
     if (!c || !host || (elem_bytes != 8 && elem_bytes != 4)) return GFC_ERR_ARG;
     GFC_CHECK(cudaSetDevice(c->dev));

@@ -781,11 +781,10 @@ extern "C" int gfc_batch_upload(gfc_batch *b, int slot, const void *host, int el
         uint32_t n = std::min<uint32_t>(per, l.nt - t0);
         GFC_CHECK(cudaMemcpyAsync(sl.u64r, (const char *)host + (size_t)t0 * per_slice, n * per_slice,
                                   cudaMemcpyHostToDevice, b->s));
-        launch_load_links(sl.u64r, elem_bytes, byteswap, l, t0, n, sl.u, sl.ut, b->s);
+        // byte swap, precision, layout and reunitarisation in one pass
+        launch_load_links(sl.u64r, elem_bytes, byteswap, l, t0, n, sl.u, sl.ut, b->s, 1, b->status);
     }
-    launch_reunitarize(sl.u, l.vh, 3 * l.npar, b->status, b->s);
-    launch_reunitarize(sl.ut, l.vh, l.npar, b->status, b->s);
-    b->launches += 2 + (l.nt + per - 1) / per;
+    b->launches += (l.nt + per - 1) / per;
     GFC_CHECK(cudaGetLastError());
     return GFC_OK;
 }

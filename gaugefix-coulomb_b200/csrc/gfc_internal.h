@@ -27,8 +27,9 @@ void launch_functional(const double2 *u, const Lat &l, double *part, double *out
 // ---- layout transforms (gfc_kernels_io.cu)
 // Raw file bytes (reference AoS order, elem_bytes 8 or 4, optionally big endian)
 // for timeslices [t0, t0+nts) -> SoA FP64 spatial links u and temporal links ut.
+// (reunit != 0: each matrix projected to SU(3) as it is stored; failures set status)
 void launch_load_links(const void *raw, int elem_bytes, int swap, const Lat &l, uint32_t t0, uint32_t nts,
-                       double2 *u, double2 *ut, cudaStream_t s);
+                       double2 *u, double2 *ut, cudaStream_t s, int reunit = 0, unsigned *status = nullptr);
 // SoA FP64 G of timeslices [t0, t0+nts) -> AoS (elem_bytes 8 or 4, optional swap)
 void launch_store_gt(const double2 *g, const Lat &l, uint32_t t0, uint32_t nts, int elem_bytes, int swap,
                      void *raw, cudaStream_t s);

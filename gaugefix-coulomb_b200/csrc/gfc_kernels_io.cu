@@ -51,8 +51,12 @@ __device__ __forceinline__ void store_elem(void *raw, size_t e, int elem_bytes, 
 }
 
 // one thread per (site, mu) of the chunk; raw holds the chunk only
+// With reunit != 0 each matrix is also projected to SU(3) (projectSU3, the reference
+// arithmetic of k_reunitarize) before it is stored: loadConfig and reunitarizeField
+// (gauge_fix_coulomb.c:123-131) in one pass over the links.
 __global__ void k_load_links(const void *__restrict__ raw, int elem_bytes, int swap, Lat l, uint32_t t0,
-                             uint32_t nts, double2 *__restrict__ u, double2 *__restrict__ ut) {
+                             uint32_t nts, double2 *__restrict__ u, double2 *__restrict__ ut, int reunit,
+                             unsigned *__restrict__ status) {
     size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     size_t nmat = (size_t)nts * l.vs * 4;
     if (k >= nmat) return;
@@ -60,18 +64,22 @@ __global__ void k_load_links(const void *__restrict__ raw, int elem_bytes, int s
     int mu = (int)(k & 3);
     Slot s = slot_of(l, L);
     double2 *dst = mu == 0 ? ut + gidx(l, s.par, 0, s.i) : u + uidx(l, mu - 1, s.par, 0, s.i);
+    M3 m;
 #pragma unroll
     for (int c = 0; c < 9; c++) {
         double re = load_elem(raw, k * 18 + 2 * c, elem_bytes, swap);
         double im = load_elem(raw, k * 18 + 2 * c + 1, elem_bytes, swap);
-        dst[(size_t)c * l.vh] = make_double2(re, im);
+        m.e[c] = make_double2(re, im);
     }
+    if (reunit && xproject(m)) atomicOr(status, GFC_STATUS_PROJECT_FAIL);
+    store_m(dst, l.vh, m);
 }
 
 void launch_load_links(const void *raw, int elem_bytes, int swap, const Lat &l, uint32_t t0, uint32_t nts,
-                       double2 *u, double2 *ut, cudaStream_t s) {
+                       double2 *u, double2 *ut, cudaStream_t s, int reunit, unsigned *status) {
     size_t n = (size_t)nts * l.vs * 4;
-    k_load_links<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(raw, elem_bytes, swap, l, t0, nts, u, ut);
+    k_load_links<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(raw, elem_bytes, swap, l, t0, nts, u, ut, reunit,
+                                                               status);
 }
 
 __global__ void k_store_gt(const double2 *__restrict__ g, Lat l, uint32_t t0, uint32_t nts, int elem_bytes,

@@ -124,6 +124,7 @@ def _load():
         "gfc_ctx_finalize_temporal": (I, [P]),
         "gfc_ctx_fix": (I, [P, ctypes.POINTER(Params), ctypes.POINTER(Options), ctypes.POINTER(Report)]),
         "gfc_ctx_apply_gt": (I, [P]),
+        "gfc_ctx_upload_links_reunit": (I, [P, P, I, I]),
         "gfc_gaugefix_overrelaxation": (I, [I, I, P, P, ctypes.POINTER(Params), ctypes.POINTER(Options),
                                             ctypes.POINTER(Report), I]),
         "gfc_e2_theta_device_noalloc": (I, [I, I, P, P, DP, DP]),
@@ -233,6 +234,12 @@ class Lattice:
         a = np.ascontiguousarray(buf)
         assert a.nbytes == self.V * 4 * 18 * elem_bytes, "link buffer size"
         _check(lib.gfc_ctx_upload_links(self.h, a.ctypes.data, elem_bytes, int(byteswap)), "upload_links")
+
+    def upload_links_reunit(self, buf, elem_bytes=8, byteswap=False):
+        """upload_links + reunitarize in one pass over the links."""
+        a = np.ascontiguousarray(buf)
+        assert a.nbytes == self.V * 4 * 18 * elem_bytes, "link buffer size"
+        _check(lib.gfc_ctx_upload_links_reunit(self.h, a.ctypes.data, elem_bytes, int(byteswap)), "upload_links_reunit")
 
     def download_links(self, elem_bytes=8, byteswap=False, out=None):
         dt = np.float64 if elem_bytes == 8 else np.float32

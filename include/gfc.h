@@ -159,6 +159,9 @@ int  gfc_ctx_sync(gfc_ctx *c);
  * big-endian files (NEED_BYTE_SWAP_IN).  Pinned host memory is copied directly;
  * other memory goes through pinned staging.  Swap and conversion run on the GPU. */
 int  gfc_ctx_upload_links(gfc_ctx *c, const void *host, int elem_bytes, int byteswap);
+/* loadConfig + reunitarizeField (gauge_fix_coulomb.c:123-131) fused: the links as
+ * gfc_ctx_upload_links then gfc_ctx_reunitarize give them, in one pass */
+int  gfc_ctx_upload_links_reunit(gfc_ctx *c, const void *host, int elem_bytes, int byteswap);
 int  gfc_ctx_download_links(gfc_ctx *c, void *host, int elem_bytes, int byteswap);
 int  gfc_ctx_upload_gt(gfc_ctx *c, const void *host, int elem_bytes, int byteswap);
 int  gfc_ctx_download_gt(gfc_ctx *c, void *host, int elem_bytes, int byteswap);

@@ -159,3 +159,17 @@ def test_warm_start_refused_on_the_mixed_path():
         lat.upload_links(gfc.synth_config(4, 4, 135, 0.5), 8, False)
         with pytest.raises(gfc.GFCError):
             lat.fix(gfc.default_params(), gfc.options(precision=gfc.PREC_MIXED, warm_start=1))
+
+
+@pytest.mark.parametrize("elem_bytes,swap", [(8, True), (4, True), (8, False)])
+def test_fused_upload_and_reunitarise(elem_bytes, swap):
+    """Loading and reunitarising in one pass gives the links of the two separate steps,
+    bit for bit."""
+    ns, nt = 4, 6
+    U = gfc.synth_config(ns, nt, 141, 0.6)
+    raw = U.astype((">" if swap else "<") + ("f4" if elem_bytes == 4 else "f8"))
+    with gfc.Lattice(ns, nt) as a, gfc.Lattice(ns, nt) as b:
+        a.upload_links(raw, elem_bytes, swap)
+        a.reunitarize()
+        b.upload_links_reunit(raw, elem_bytes, swap)
+        assert a.download_links().tobytes() == b.download_links().tobytes()
