@@ -601,34 +601,80 @@ static int fix_reference_schedule(gfc_ctx *c, const gfc_params *p, const gfc_opt
 
 // Exact kernel with the proxy evaluated after every half-sweep (standalone
 // reduction, one host wait per half-sweep): reference arithmetic, earliest stop.
+// Reference arithmetic, the proxy measured exactly (as calculate_e2 / calculateTheta
+// do), near the tolerance after every half-sweep.  The test runs on the device: a check kernel after each
+// half-sweep's observables sets a stop word, after which the queued sweep and
+// observables launches do nothing, so the links returned are those whose proxy was
+// found below the tolerance.  The host reads the stop word every 32 half-sweeps and
+// reunitarises at the reunitarisation period, which always ends a chunk.
 static int fix_every_sweep_exact(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report *r) {
     const double omega = (double)p->omega_OR;
     const Lat &l = c->lat;
-    int sweep = 0, rc = GFC_FIX_NOT_CONVERGED;
+    int sweep = 0;
     double res;
     int e = proxy(c, p, &res);
     if (e) return e;
     r->initial_residue = res;
     if (o->verbose) print_res(sweep, res);
     GFC_CHECK(cudaEventRecord(c->ev_b, c->s));
-    if (res <= p->tolerance) rc = 0;
-    while (rc != 0 && sweep < (int)p->max_sweeps_to_fix) {
-        launch_sweep_exact(c->u, c->g, l, sweep, omega, p->hits, c->s, c->shape_exact);
-        c->launches++;
-        sweep++;
-        e = proxy(c, p, &res);
-        if (e) return e;
-        if (res <= p->tolerance) {
-            rc = 0;
-            r->first_below_tol = sweep;
-            break;
+    if (res <= p->tolerance) {
+        GFC_CHECK(cudaEventRecord(c->ev_d, c->s));
+        r->sweeps = 0;
+        r->first_below_tol = 0;
+        return 0;
+    }
+    unsigned *stop = c->tickets + (l.nt + 1);
+    GFC_CHECK(cudaMemsetAsync(stop, 0, sizeof(unsigned), c->s));
+    const int theta = p->gfix_proxy == GFC_PROXY_THETA;
+    const int max = (int)p->max_sweeps_to_fix, period = (int)p->sweeps_to_reunitarization;
+    // The proxy is measured at the end of each chunk while it and its rate put the
+    // tolerance more than two chunks away (or it is above 1e3 x tolerance), and after
+    // every half-sweep from then on (dense_check: always): the measuring pass costs
+    // about as much as a half-sweep.
+    unsigned hstop = 0;
+    bool dense = o->dense_check != 0;
+    int k_a = -1;
+    double res_a = 0.0;
+    while (sweep < max) {
+        int end = std::min(max, sweep + 32);
+        if (period > 0) end = std::min(end, (sweep / period + 1) * period);
+        for (; sweep < end; sweep++) {
+            launch_sweep_exact(c->u, c->g, l, sweep, omega, p->hits, c->s, c->shape_exact, stop);
+            c->launches++;
+            if (dense || sweep + 1 == end) {
+                launch_obs(c->u, l, c->part, c->dres, nullptr, c->s, stop);
+                launch_exact_check(c->dres, l, theta, p->tolerance, sweep + 1, stop, c->s);
+                c->launches += 3;
+            }
         }
-        if (!(sweep % p->sweeps_to_reunitarization)) reunit_spatial_and_g(c);
+        GFC_CHECK(cudaMemcpyAsync(c->hres + 16, stop, sizeof(unsigned), cudaMemcpyDeviceToHost, c->s));
+        GFC_CHECK(cudaMemcpyAsync(c->hres + 20, c->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        GFC_CHECK(cudaStreamSynchronize(c->s));
+        GFC_CHECK(cudaGetLastError());
+        memcpy(&hstop, c->hres + 16, sizeof hstop);
+        if (hstop) break;
+        if (!dense) {
+            const double res_k = theta ? c->hres[21] / (3.0 * (double)l.v) : c->hres[20] / (double)l.v;
+            if (!(res_k == res_k)) break;   // NaN: reported by the final observables
+            if (res_k <= 1e3 * p->tolerance) {
+                dense = true;
+            } else if (k_a >= 0 && res_k < res_a) {
+                const double rate = pow(res_k / res_a, 1.0 / (double)(sweep - k_a));
+                if (res_k * pow(rate, 64.0) <= 10.0 * p->tolerance) dense = true;
+            }
+            k_a = sweep;
+            res_a = res_k;
+        }
+        if (period > 0 && !(sweep % period)) reunit_spatial_and_g(c);
     }
     GFC_CHECK(cudaEventRecord(c->ev_d, c->s));
+    if (hstop) {
+        sweep = (int)hstop;
+        r->first_below_tol = sweep;
+    }
     r->sweeps = sweep;
     r->site_updates = (long long)sweep * (l.cb ? l.vh : l.v / 2);
-    return rc == 0 ? sweep : rc;
+    return hstop ? sweep : GFC_FIX_NOT_CONVERGED;
 }
 
 extern "C" void gfc_options_default(gfc_options *o) {

@@ -15,13 +15,18 @@ struct gfc_batch;
 namespace gfc {
 
 // ---- exact FP64 kernels (gfc_kernels_exact.cu)
+// stop (optional): a device stop word; once set, the launch does nothing
 void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
-                        cudaStream_t s, int shape = 0);
+                        cudaStream_t s, int shape = 0, const unsigned *stop = nullptr);
 int exact_num_shapes();
 void launch_reunitarize(double2 *base, uint32_t stride, uint32_t nblk, unsigned *status, cudaStream_t s);
 void launch_identity(double2 *g, const Lat &l, cudaStream_t s);
 int obs_blocks_per_slice(const Lat &l);
-void launch_obs(const double2 *u, const Lat &l, double *part, double *out, double *slice_out, cudaStream_t s);
+void launch_obs(const double2 *u, const Lat &l, double *part, double *out, double *slice_out, cudaStream_t s,
+                const unsigned *stop = nullptr);
+// proxy of out (launch_obs) <= tol sets *stop = sweep (once)
+void launch_exact_check(const double *out, const Lat &l, int theta, double tol, int sweep, unsigned *stop,
+                        cudaStream_t s);
 void launch_functional(const double2 *u, const Lat &l, double *part, double *out, cudaStream_t s);
 
 // ---- layout transforms (gfc_kernels_io.cu)

@@ -63,9 +63,12 @@ __device__ __forceinline__ void site_update_exact(double2 *__restrict__ u, doubl
 
 // Launch shapes (threads per block, minimum resident blocks per SM); the second
 // caps registers per thread.  gfc_ctx_autotune picks one per lattice.
+// stop (may be null): a stop word set on the device; once it is, the launch does nothing
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_exact(double2 *__restrict__ u, double2 *__restrict__ g,
-                                                             Lat l, int par, double omega, unsigned hits) {
+                                                             Lat l, int par, double omega, unsigned hits,
+                                                             const unsigned *stop) {
+    if (stop && *(volatile const unsigned *)stop) return;
     uint32_t i = blockIdx.x * BLOCK + threadIdx.x;
     if (i >= l.vh) return;
     Coord c = coord_cb(l, par, i);
@@ -139,8 +142,10 @@ __device__ __forceinline__ void site_update_exact_staged(double2 *__restrict__ u
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_exact_staged(double2 *__restrict__ u,
                                                                     double2 *__restrict__ g, Lat l, int par,
-                                                                    double omega, unsigned hits) {
+                                                                    double omega, unsigned hits,
+                                                                    const unsigned *stop) {
     extern __shared__ __align__(16) unsigned char exact_stage[];
+    if (stop && *(volatile const unsigned *)stop) return;
     uint32_t i = blockIdx.x * BLOCK + threadIdx.x;
     if (i >= l.vh) return;
     Coord c = coord_cb(l, par, i);
@@ -149,7 +154,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_exact_staged(double2 *__r
 
 template <int BLOCK, int MINB>
 static void launch_exact_staged(const Lat &l, double2 *u, double2 *g, int par, double omega, unsigned hits,
-                                cudaStream_t s) {
+                                cudaStream_t s, const unsigned *stop) {
     constexpr size_t bytes = (size_t)6 * 9 * BLOCK * sizeof(double2);
     static_assert(bytes <= 227 * 1024, "staged links exceed shared memory");
     auto kern = k_sweep_exact_staged<BLOCK, MINB>;
@@ -161,14 +166,15 @@ static void launch_exact_staged(const Lat &l, double2 *u, double2 *g, int par, d
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         done |= 1ull << dev;
     }
-    kern<<<(l.vh + BLOCK - 1) / BLOCK, BLOCK, bytes, s>>>(u, g, l, par, omega, hits);
+    kern<<<(l.vh + BLOCK - 1) / BLOCK, BLOCK, bytes, s>>>(u, g, l, par, omega, hits, stop);
 }
 
 // Odd ns: same-parity sites meet across the periodic boundary, so updates inside
 // a timeslice depend on their order.  One thread per timeslice visits the slice in
 // the reference's z, y, x order; distinct timeslices share no spatial link.
 __global__ void k_sweep_exact_serial(double2 *__restrict__ u, double2 *__restrict__ g, Lat l, int sweep,
-                                     double omega, unsigned hits) {
+                                     double omega, unsigned hits, const unsigned *stop) {
+    if (stop && *(volatile const unsigned *)stop) return;
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (uint32_t)l.nt) return;
     for (uint32_t r = 0; r < l.vs; r++) {
@@ -181,29 +187,29 @@ __global__ void k_sweep_exact_serial(double2 *__restrict__ u, double2 *__restric
 int exact_num_shapes() { return 5; }
 
 void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
-                        cudaStream_t s, int shape) {
+                        cudaStream_t s, int shape, const unsigned *stop) {
     if (l.cb) {
         int par = sweep & 1;  // BLACKRED_SWEEP: even sites on even sweeps (gauge_fixing.c:42)
         switch (shape) {
             case 1:
-                k_sweep_exact<128, 3><<<(l.vh + 127) / 128, 128, 0, s>>>(u, g, l, par, omega, hits);
+                k_sweep_exact<128, 3><<<(l.vh + 127) / 128, 128, 0, s>>>(u, g, l, par, omega, hits, stop);
                 break;
             case 2:
-                k_sweep_exact<64, 4><<<(l.vh + 63) / 64, 64, 0, s>>>(u, g, l, par, omega, hits);
+                k_sweep_exact<64, 4><<<(l.vh + 63) / 64, 64, 0, s>>>(u, g, l, par, omega, hits, stop);
                 break;
             case 3:   // 110.6 KiB of staged links per CTA, 2 CTAs per SM
-                launch_exact_staged<128, 2>(l, u, g, par, omega, hits, s);
+                launch_exact_staged<128, 2>(l, u, g, par, omega, hits, s, stop);
                 break;
             case 4:   // 55.3 KiB per CTA, 4 CTAs per SM
-                launch_exact_staged<64, 4>(l, u, g, par, omega, hits, s);
+                launch_exact_staged<64, 4>(l, u, g, par, omega, hits, s, stop);
                 break;
             default:
-                k_sweep_exact<128, 1><<<(l.vh + 127) / 128, 128, 0, s>>>(u, g, l, par, omega, hits);
+                k_sweep_exact<128, 1><<<(l.vh + 127) / 128, 128, 0, s>>>(u, g, l, par, omega, hits, stop);
                 break;
         }
     } else {
         unsigned blocks = (l.nt + 31) / 32;
-        k_sweep_exact_serial<<<blocks, 32, 0, s>>>(u, g, l, sweep, omega, hits);
+        k_sweep_exact_serial<<<blocks, 32, 0, s>>>(u, g, l, sweep, omega, hits, stop);
     }
 }
 
@@ -342,7 +348,8 @@ __device__ __forceinline__ void block_sum(double (&v)[NQ]) {
 
 // grid (nbx, nt): block bx of slice t sums sites of both parities of slice t
 __global__ void __launch_bounds__(256) k_obs_partials(const double2 *__restrict__ u, Lat l,
-                                                      double *__restrict__ part) {
+                                                      double *__restrict__ part, const unsigned *stop) {
+    if (stop && *(volatile const unsigned *)stop) return;
     const uint32_t t = blockIdx.y;
     const uint32_t vsh = l.cb ? l.vs / 2 : l.vs;  // slots of one parity per slice
     const uint32_t n = vsh * l.npar;
@@ -392,7 +399,8 @@ __global__ void __launch_bounds__(256) k_functional_partials(const double2 *__re
 // Sum partials [nt][nbx][nq] per slice in a fixed order, then the slices.
 // out[q] = total, slice_out[t*nq + q] = per slice (optional).
 __global__ void k_finalize(const double *__restrict__ part, int nt, int nbx, int nq, double *__restrict__ out,
-                           double *__restrict__ slice_out) {
+                           double *__restrict__ slice_out, const unsigned *stop) {
+    if (stop && *(volatile const unsigned *)stop) return;
     __shared__ double acc[4][256];
     for (int q = 0; q < nq; q++) acc[q][threadIdx.x] = 0.0;
     for (int t = threadIdx.x; t < nt; t += blockDim.x) {
@@ -424,16 +432,32 @@ int obs_blocks_per_slice(const Lat &l) {
     return nb;
 }
 
-void launch_obs(const double2 *u, const Lat &l, double *part, double *out, double *slice_out, cudaStream_t s) {
+void launch_obs(const double2 *u, const Lat &l, double *part, double *out, double *slice_out, cudaStream_t s,
+                const unsigned *stop) {
     int nbx = obs_blocks_per_slice(l);
-    k_obs_partials<<<dim3(nbx, l.nt), 256, 0, s>>>(u, l, part);
-    k_finalize<<<1, 256, 0, s>>>(part, l.nt, nbx, 2, out, slice_out);
+    k_obs_partials<<<dim3(nbx, l.nt), 256, 0, s>>>(u, l, part, stop);
+    k_finalize<<<1, 256, 0, s>>>(part, l.nt, nbx, 2, out, slice_out, stop);
+}
+
+// After the observables of half-sweep `sweep`: the proxy (e2 = out[0] / V, or theta =
+// out[1] / 3V, normalised as the host does) below the tolerance sets the stop word to
+// sweep, once; later sweep and observables launches of the stream then do nothing.
+__global__ void k_exact_check(const double *__restrict__ out, double v, int theta, double tol, int sweep,
+                              unsigned *stop) {
+    if (threadIdx.x || blockIdx.x || *(volatile unsigned *)stop) return;
+    const double res = theta ? out[1] / (3.0 * v) : out[0] / v;
+    if (res <= tol) *stop = (unsigned)sweep;
+}
+
+void launch_exact_check(const double *out, const Lat &l, int theta, double tol, int sweep, unsigned *stop,
+                        cudaStream_t s) {
+    k_exact_check<<<1, 32, 0, s>>>(out, (double)l.v, theta, tol, sweep, stop);
 }
 
 void launch_functional(const double2 *u, const Lat &l, double *part, double *out, cudaStream_t s) {
     int nbx = obs_blocks_per_slice(l);
     k_functional_partials<<<dim3(nbx, l.nt), 256, 0, s>>>(u, l, part);
-    k_finalize<<<1, 256, 0, s>>>(part, l.nt, nbx, 1, out, nullptr);
+    k_finalize<<<1, 256, 0, s>>>(part, l.nt, nbx, 1, out, nullptr, nullptr);
 }
 
 }  // namespace gfc

@@ -157,7 +157,8 @@ def test_slice_blocking_same_results():
         assert rc2 > 0 and r2.final_residue <= 1e-15
 
 
-@pytest.mark.parametrize("precision", [gfc.PREC_FP64_FAST, gfc.PREC_MIXED, gfc.PREC_FP64_FULL])
+@pytest.mark.parametrize("precision", [gfc.PREC_FP64_FAST, gfc.PREC_MIXED, gfc.PREC_FP64_FULL,
+                                       gfc.PREC_FP64_EXACT])
 def test_sparse_e2_measurement_stops_at_the_same_half_sweep(precision):
     """Measuring e2 only on one pair of half-sweeps per chunk while the tolerance is
     far must not change the stop: same first half-sweep below tolerance, same G."""
