@@ -258,7 +258,13 @@ __device__ __forceinline__ void fupdate(Mt<T> &w, T omega, unsigned hits, Mt<T> 
         fsub_hit<1, 2>(w, g);
     }
 #pragma unroll 1
-    for (unsigned h = 1; h < hits; h++) {
+    for (unsigned h = 1; h + 1 < hits; h++) {
+        fsub_hit<0, 1>(w, g);
+        fsub_hit<0, 2>(w, g);
+        fsub_hit<1, 2>(w, g);
+    }
+    if (hits > 1) {   // the last hit written out: the entries of w that no later
+                      // coefficient reads are not computed
         fsub_hit<0, 1>(w, g);
         fsub_hit<0, 2>(w, g);
         fsub_hit<1, 2>(w, g);
