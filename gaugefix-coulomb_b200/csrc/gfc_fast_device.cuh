@@ -46,14 +46,19 @@ template <typename C>
 __device__ __forceinline__ C fconj(C a) {
     return mkc<C>(a.x, -a.y);
 }
-// s + a b and s + a conj(b)
+// s + a b, s + a conj(b) and s - a b as chains of fused multiply-adds (four per
+// complex product instead of two products, two fused operations and two sums)
 template <typename C>
 __device__ __forceinline__ C fmac(C s, C a, C b) {
-    return fadd(s, fmul(a, b));
+    return mkc<C>(fma(-a.y, b.y, fma(a.x, b.x, s.x)), fma(a.y, b.x, fma(a.x, b.y, s.y)));
 }
 template <typename C>
 __device__ __forceinline__ C fmac_conj(C s, C a, C b) {
-    return fadd(s, fmul_conj(a, b));
+    return mkc<C>(fma(a.y, b.y, fma(a.x, b.x, s.x)), fma(-a.x, b.y, fma(a.y, b.x, s.y)));
+}
+template <typename C>
+__device__ __forceinline__ C fmsub(C s, C a, C b) {
+    return mkc<C>(fma(a.y, b.y, fma(-a.x, b.x, s.x)), fma(-a.y, b.x, fma(-a.x, b.y, s.y)));
 }
 
 // FP32 complex arithmetic on paired single-precision instructions (one instruction
@@ -76,6 +81,10 @@ __device__ __forceinline__ float2 fmac_conj(float2 s, float2 a, float2 b) {
     s = __ffma2_rn(a, make_float2(b.x, b.x), s);
     return __ffma2_rn(make_float2(a.y, -a.x), make_float2(b.y, b.y), s);
 }
+__device__ __forceinline__ float2 fmsub(float2 s, float2 a, float2 b) {
+    s = __ffma2_rn(make_float2(-a.x, -a.x), b, s);
+    return __ffma2_rn(make_float2(a.y, -a.y), make_float2(b.y, b.x), s);
+}
 
 __device__ __forceinline__ double frsqrt(double x) { return rsqrt(x); }
 __device__ __forceinline__ float frsqrt(float x) { return rsqrtf(x); }
@@ -83,9 +92,9 @@ __device__ __forceinline__ float frsqrt(float x) { return rsqrtf(x); }
 // conj(a x b)
 template <typename C>
 __device__ __forceinline__ void fcross_conj(const C *a, const C *b, C *o) {
-    o[0] = fconj(fadd(fmul(a[1], b[2]), mkc<C>(-(a[2].x * b[1].x - a[2].y * b[1].y), -(a[2].x * b[1].y + a[2].y * b[1].x))));
-    o[1] = fconj(fadd(fmul(a[2], b[0]), mkc<C>(-(a[0].x * b[2].x - a[0].y * b[2].y), -(a[0].x * b[2].y + a[0].y * b[2].x))));
-    o[2] = fconj(fadd(fmul(a[0], b[1]), mkc<C>(-(a[1].x * b[0].x - a[1].y * b[0].y), -(a[1].x * b[0].y + a[1].y * b[0].x))));
+    o[0] = fconj(fmsub(fmul(a[1], b[2]), a[2], b[1]));
+    o[1] = fconj(fmsub(fmul(a[2], b[0]), a[0], b[2]));
+    o[2] = fconj(fmsub(fmul(a[0], b[1]), a[1], b[0]));
 }
 
 template <typename T>
@@ -191,32 +200,73 @@ __device__ __forceinline__ double e2_from_w(const Mt<T> &w) {
     return c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4 + c5 * c5 + c6 * c6 + c7 * c7 + c8 * c8;
 }
 
-// one Cabibbo-Marinari hit on rows (A, B) of w, accumulated into g
+// Cabibbo-Marinari coefficients of the SU(2) subgroup on rows (A, B) of w: the
+// embedded unit quaternion as x = {x_AA, x_AB, x_BA, x_BB}; false when the 2x2 block
+// gives no direction (the hit is then the identity)
 template <int A, int B, typename T>
-__device__ __forceinline__ void fsub_hit(Mt<T> &w, Mt<T> &g) {
+__device__ __forceinline__ bool fsub_coef(const Mt<T> &w, typename CT<T>::t (&x)[4]) {
     using C = typename CT<T>::t;
     T k0 = w.e[EL(A, A)].x + w.e[EL(B, B)].x;
     T k1 = -(w.e[EL(A, B)].y + w.e[EL(B, A)].y);
     T k2 = -(w.e[EL(A, B)].x - w.e[EL(B, A)].x);
     T k3 = -(w.e[EL(A, A)].y - w.e[EL(B, B)].y);
     T n = k0 * k0 + k1 * k1 + k2 * k2 + k3 * k3;
-    if (n == T(0)) return;
+    if (n == T(0)) return false;
     T r = frsqrt(n);
     k0 *= r;
     k1 *= r;
     k2 *= r;
     k3 *= r;
-    const C x00 = mkc<C>(k0, k3), x01 = mkc<C>(k2, k1), x10 = mkc<C>(-k2, k1), x11 = mkc<C>(k0, -k3);
+    x[0] = mkc<C>(k0, k3);
+    x[1] = mkc<C>(k2, k1);
+    x[2] = mkc<C>(-k2, k1);
+    x[3] = mkc<C>(k0, -k3);
+    return true;
+}
+// rows (A, B) of m <- x . rows (A, B) of m
+template <int A, int B, typename T>
+__device__ __forceinline__ void frot_rows(Mt<T> &m, const typename CT<T>::t (&x)[4]) {
+    using C = typename CT<T>::t;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        C a = w.e[EL(A, c)], b = w.e[EL(B, c)];
-        w.e[EL(A, c)] = fmac(fmul(x00, a), x01, b);
-        w.e[EL(B, c)] = fmac(fmul(x10, a), x11, b);
-        a = g.e[EL(A, c)];
-        b = g.e[EL(B, c)];
-        g.e[EL(A, c)] = fmac(fmul(x00, a), x01, b);
-        g.e[EL(B, c)] = fmac(fmul(x10, a), x11, b);
+        const C a = m.e[EL(A, c)], b = m.e[EL(B, c)];
+        m.e[EL(A, c)] = fmac(fmul(x[0], a), x[1], b);
+        m.e[EL(B, c)] = fmac(fmul(x[2], a), x[3], b);
     }
+}
+// one Cabibbo-Marinari hit on rows (A, B) of w, accumulated into g
+template <int A, int B, typename T>
+__device__ __forceinline__ void fsub_hit(Mt<T> &w, Mt<T> &g) {
+    typename CT<T>::t x[4];
+    if (!fsub_coef<A, B>(w, x)) return;
+    frot_rows<A, B>(w, x);
+    frot_rows<A, B>(g, x);
+}
+// the first hit, starting from g = 1: the product of the three embedded subgroup
+// elements is written out, without the products with the zeros and ones of the
+// identity (which IEEE arithmetic does not let the compiler drop)
+template <typename T>
+__device__ __forceinline__ void fhit_first(Mt<T> &w, Mt<T> &g) {
+    using C = typename CT<T>::t;
+    C r[4], s[4], t[4];
+    const C one = mkc<C>(T(1), T(0)), zero = mkc<C>(T(0), T(0));
+    if (!fsub_coef<0, 1>(w, r)) r[0] = one, r[1] = zero, r[2] = zero, r[3] = one;
+    frot_rows<0, 1>(w, r);
+    if (!fsub_coef<0, 2>(w, s)) s[0] = one, s[1] = zero, s[2] = zero, s[3] = one;
+    frot_rows<0, 2>(w, s);
+    if (!fsub_coef<1, 2>(w, t)) t[0] = one, t[1] = zero, t[2] = zero, t[3] = one;
+    frot_rows<1, 2>(w, t);
+    // R = [[r0 r1 0] [r2 r3 0] [0 0 1]]; S acts on rows 0, 2; T on rows 1, 2
+    const C g20 = fmul(s[2], r[0]), g21 = fmul(s[2], r[1]);
+    g.e[0] = fmul(s[0], r[0]);
+    g.e[1] = fmul(s[0], r[1]);
+    g.e[2] = s[1];
+    g.e[3] = fmac(fmul(t[0], r[2]), t[1], g20);
+    g.e[4] = fmac(fmul(t[0], r[3]), t[1], g21);
+    g.e[5] = fmul(t[1], s[3]);
+    g.e[6] = fmac(fmul(t[2], r[2]), t[3], g20);
+    g.e[7] = fmac(fmul(t[2], r[3]), t[3], g21);
+    g.e[8] = fmul(t[3], s[3]);
 }
 
 template <typename T>
@@ -250,13 +300,10 @@ __device__ __forceinline__ void fidentity(Mt<T> &m) {
 template <typename T>
 __device__ __forceinline__ void fupdate(Mt<T> &w, T omega, unsigned hits, Mt<T> &g) {
     using C = typename CT<T>::t;
-    fidentity(g);
-    if (hits > 0) {   // the first hit written out: g is still the identity, so the
-                      // compiler drops the products with its zeros and ones
-        fsub_hit<0, 1>(w, g);
-        fsub_hit<0, 2>(w, g);
-        fsub_hit<1, 2>(w, g);
-    }
+    if (hits > 0)
+        fhit_first(w, g);
+    else
+        fidentity(g);
 #pragma unroll 1
     for (unsigned h = 1; h + 1 < hits; h++) {
         fsub_hit<0, 1>(w, g);
