@@ -43,9 +43,9 @@ struct gfc_ctx {
     // launch shapes of the sweep kernels (indices into the compiled shape tables;
     // defaults until gfc_ctx_autotune measures them for this lattice)
     // (the defaults are the shapes measured fastest at 32^3x64 on a B200: exact with
-    // staged links 128x2, fast FP64 staged 128x3, FP32 plain 128x5)
+    // staged links 128x2, fast FP64 staged in blocks of 32 sites, FP32 plain 128x5)
     int shape_exact = 3;
-    int shape_fast64 = 11;
+    int shape_fast64 = 13;
     int shape_fast32 = 7;
     int tuned = 0;
     // slice blocking of the fast sweeps: groups of blk*_slices timeslices run

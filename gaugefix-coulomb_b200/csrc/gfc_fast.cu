@@ -77,13 +77,13 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 struct SShape {
     int block, minb, sg, nst;   // nst: links staged per site (whole directions: 2, 4 or 6)
 };
-constexpr SShape kStaged[] = {{128, 2, 1, 6}, {64, 5, 1, 6}, {128, 3, 0, 6}, {256, 1, 1, 6}, {128, 4, 1, 6},
-                              {128, 5, 1, 6}, {128, 4, 0, 4}, {64, 6, 0, 4}, {128, 5, 0, 2}};
+constexpr SShape kStaged[] = {{128, 2, 1, 6}, {64, 5, 1, 6}, {128, 3, 0, 6}, {64, 6, 0, 6}, {32, 11, 0, 6},
+                              {64, 7, 0, 4}, {128, 4, 0, 4}, {64, 6, 0, 4}, {128, 4, 0, 2}};
 constexpr int kNumStaged = sizeof(kStaged) / sizeof(kStaged[0]);
 constexpr int kNumAll = kNumShapes + kNumStaged;   // shape indices: plain, then staged
 constexpr int kNE = 5;   // exact-kernel shapes (gfc_kernels_exact.cu)
 static_assert(kNE + 2 * kNumAll + 8 == GFC_TUNE_SLOTS, "autotune time slots");
-constexpr int MIN_BLOCK = 64;   // smallest block: sizes the per-block partial buffers
+constexpr int MIN_BLOCK = 32;   // smallest block: sizes the per-block partial buffers
 
 // deterministic sum of NQ values over the block; result in thread 0
 template <int BLOCK, int NQ>
@@ -355,6 +355,7 @@ static TrackPtrs track_ptrs(gfc_ctx *c) {
 template <class S, int K>
 static void launch_shape(dim3 grid, cudaStream_t st, typename S::V *u, typename S::V *g, const SweepArgs &a) {
     constexpr int B = kShapes[K].block;
+    static_assert(B >= MIN_BLOCK, "block partial buffers are sized for MIN_BLOCK");
     grid.x = ((a.l.vs >> 1) + B - 1) / B;
     k_sweep_fast<S, B, kShapes[K].minb><<<grid, B, 0, st>>>(u, g, a);
 }
@@ -369,6 +370,7 @@ static void launch_staged(dim3 grid, cudaStream_t st, typename S::V *u, typename
     constexpr SShape sh = kStaged[K];
     constexpr size_t bytes = staged_bytes<S>(sh.block, sh.sg, sh.nst);
     static_assert(bytes <= 227 * 1024, "staged tile exceeds shared memory");
+    static_assert(sh.block >= MIN_BLOCK, "block partial buffers are sized for MIN_BLOCK");
     auto kern = k_sweep_staged<S, sh.block, sh.minb, (bool)sh.sg, sh.nst>;
     // the attribute is set once per device (a CUDA function attribute is per context)
     static unsigned long long done = 0;
@@ -811,7 +813,7 @@ extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
     int rc = gfc_ctx_save_links(c);
     if (rc) return rc;
     const Lat &l = c->lat;
-    const int n = 6;
+    const int n = 10;
     rc = ensure_track_buffers(c, 2 * n + 2);
     if (rc) return rc;
     TrackPtrs tp = track_ptrs(c);
@@ -832,7 +834,7 @@ extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
         a.par = sweep & 1;
         a.omega = 1.95;
         a.hits = 2;
-        a.track = 1;
+        a.track = 0;   // as most launches of a fix: e2 is measured on a few of them
         a.t0 = 0;
         a.ring = c->ring;
         a.ring_n = c->ring_n;
