@@ -59,6 +59,9 @@ def parse_args():
     p.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrival rate per second")
     p.add_argument("--batch-mix", default="16x32:32,24x48:32,32x64:32",
                    help="batch run: comma list of NSxNT:count (default: the 96-config mix)")
+    p.add_argument("--shapes", default="",
+                   help="exact,fp64,fp32 launch-shape indices to use instead of autotuning (to profile the "
+                        "shapes the autotuner picks when no profiler slows its trial launches)")
     p.add_argument("--only", default="", help="comma list of batch,serve: run just those (no headline line)")
     return p.parse_args()
 
@@ -184,7 +187,11 @@ def run_gfc(a, rk):
     lat.reunitarize()
     lat.save_links()
     # one-time per-lattice choice of launch shapes (not part of a step)
-    tune = lat.autotune()
+    if a.shapes:
+        lat.set_shapes(*[int(x) for x in a.shapes.split(",")])
+        tune = None
+    else:
+        tune = lat.autotune()
     params = gfc.default_params(tolerance=a.tol)
     fast = gfc.options(precision=gfc.PREC_FP64_FAST, stop_rule=gfc.STOP_EVERY)
     stream = torch.cuda.ExternalStream(lat.stream, device=f"cuda:{rk.local}")

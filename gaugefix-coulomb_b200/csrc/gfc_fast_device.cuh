@@ -748,6 +748,20 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
         S::store(g + sg_idx<S>(l, par, i), l.vh, o);
     }
     double cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if constexpr (ND == 3) {
+        // one copy of the direction body: the fully unrolled form outgrows the
+        // instruction cache when many small blocks share an SM (3 % slower with
+        // 32-site blocks); the operands come from shared memory, so the rolled loop
+        // loses no load parallelism
+#pragma unroll 1
+        for (int d = 0; d < 3; d++) {
+            const uint32_t b = d == 0 ? ib[0] : (d == 1 ? ib[1] : ib[2]);
+            apply_staged<S, true>(my + (2 * d) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, par, i), l.vh, up, track,
+                                  cc);
+            apply_staged<S, false>(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, op, b), l.vh, up,
+                                   track, cc);
+        }
+    } else
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         if (d < ND) {
