@@ -105,10 +105,13 @@ __device__ __forceinline__ void site_update_exact_staged(double2 *__restrict__ u
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 
+    // The direction loops stay rolled: one copy of each body keeps the kernel within
+    // the instruction cache (the operands come from shared memory, so no load
+    // parallelism is lost); the arithmetic and its order are unchanged.
     M3 w;
 #pragma unroll
     for (int k = 0; k < 9; k++) w.e[k] = cz();
-#pragma unroll
+#pragma unroll 1
     for (int d = 0; d < 3; d++) {
         M3 f, r;
         load_m(my + (2 * d) * 9 * BLOCK, BLOCK, f);
@@ -128,14 +131,15 @@ __device__ __forceinline__ void site_update_exact_staged(double2 *__restrict__ u
     load_m(g + gidx(l, par, 0, si), l.vh, m);
     xprod(upd, m, t);
     store_m(g + gidx(l, par, 0, si), l.vh, t);
-#pragma unroll
+#pragma unroll 1
     for (int d = 0; d < 3; d++) {
+        const uint32_t b = d == 0 ? ib[0] : (d == 1 ? ib[1] : ib[2]);
         load_m(my + (2 * d) * 9 * BLOCK, BLOCK, m);
         xprod(upd, m, t);
         store_m(u + uidx(l, d, par, 0, si), l.vh, t);
         load_m(my + (2 * d + 1) * 9 * BLOCK, BLOCK, m);
         xprod_dag(m, upd, t);
-        store_m(u + uidx(l, d, op, 0, ib[d]), l.vh, t);
+        store_m(u + uidx(l, d, op, 0, b), l.vh, t);
     }
 }
 
@@ -194,8 +198,8 @@ void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double 
             case 1:
                 k_sweep_exact<128, 3><<<(l.vh + 127) / 128, 128, 0, s>>>(u, g, l, par, omega, hits, stop);
                 break;
-            case 2:
-                k_sweep_exact<64, 4><<<(l.vh + 63) / 64, 64, 0, s>>>(u, g, l, par, omega, hits, stop);
+            case 2:   // 27 KiB per CTA, 8 CTAs per SM
+                launch_exact_staged<32, 8>(l, u, g, par, omega, hits, s, stop);
                 break;
             case 3:   // 110.6 KiB of staged links per CTA, 2 CTAs per SM
                 launch_exact_staged<128, 2>(l, u, g, par, omega, hits, s, stop);
