@@ -3,6 +3,8 @@
 // the fused e2 components).  Shared by the single-lattice kernels (gfc_fast.cu)
 // and the batch engine (gfc_batch.cu).
 #pragma once
+#include <type_traits>
+
 #include "gfc_device.cuh"
 
 namespace gfc {
@@ -198,6 +200,25 @@ __device__ __forceinline__ double e2_from_w(const Mt<T> &w) {
     double c7 = (double)w.e[5].x - (double)w.e[7].x;
     double c8 = ((double)w.e[0].y + (double)w.e[4].y - 2.0 * (double)w.e[8].y) * 0.57735026918962576451;
     return c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4 + c5 * c5 + c6 * c6 + c7 * c7 + c8 * c8;
+}
+
+// e2 density of a site after its update: in a half-sweep the six links of x change
+// only through x's own update, so w(x) afterwards is up . w(x) before it.  Used for
+// FP64 storage, where it replaces the row-by-row accumulation from the six updated
+// links (a third of the arithmetic); FP32 keeps the accumulation.
+template <typename T>
+__device__ __forceinline__ double e2_after(const Mt<T> &up, const Mt<T> &w0) {
+    using C = typename CT<T>::t;
+    Mt<T> wn;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            C v = fmul(up.e[EL(a, 0)], w0.e[EL(0, b)]);
+            v = fmac(v, up.e[EL(a, 1)], w0.e[EL(1, b)]);
+            wn.e[EL(a, b)] = fmac(v, up.e[EL(a, 2)], w0.e[EL(2, b)]);
+        }
+    return e2_from_w(wn);
 }
 
 // Cabibbo-Marinari coefficients of the SU(2) subgroup on rows (A, B) of w: the
@@ -557,9 +578,13 @@ __device__ __forceinline__ void fast_site(typename S::V *__restrict__ u, typenam
             for (int y = 0; y < 3; y++) w.e[EL(x, y)] = fadd(w.e[EL(x, y)], fadd(f.e[EL(x, y)], fconj(r.e[EL(y, x)])));
     }
     if (track) pre = e2_from_w(w);
+    constexpr bool kPostW = std::is_same<T, double>::value;
+    Mt<T> w0;
+    if (kPostW && track) w0 = w;
 
     Mt<T> up;
     fupdate(w, omega, hits, up);
+    const int track_links = kPostW ? 0 : track;
 
     // G(x) <- up G(x)
     {
@@ -573,13 +598,17 @@ __device__ __forceinline__ void fast_site(typename S::V *__restrict__ u, typenam
     double cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        apply_forward<S>(u + su_idx<S>(l, d, par, i), l.vh, up, track, cc);
-        apply_backward<S>(u + su_idx<S>(l, d, op, ib[d]), l.vh, up, track, cc);
+        apply_forward<S>(u + su_idx<S>(l, d, par, i), l.vh, up, track_links, cc);
+        apply_backward<S>(u + su_idx<S>(l, d, op, ib[d]), l.vh, up, track_links, cc);
     }
     if (track) {
-        cc[7] *= 0.57735026918962576451;
+        if constexpr (kPostW) {
+            post = e2_after(up, w0);
+        } else {
+            cc[7] *= 0.57735026918962576451;
 #pragma unroll
-        for (int k = 0; k < 8; k++) post += cc[k] * cc[k];
+            for (int k = 0; k < 8; k++) post += cc[k] * cc[k];
+        }
     }
 }
 
@@ -732,9 +761,13 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
             for (int y = 0; y < 3; y++) w.e[EL(x, y)] = fadd(w.e[EL(x, y)], fadd(f.e[EL(x, y)], fconj(r.e[EL(y, x)])));
     }
     if (track) pre = e2_from_w(w);
+    constexpr bool kPostW = std::is_same<T, double>::value;
+    Mt<T> w0;
+    if (kPostW && track) w0 = w;
 
     Mt<T> up;
     fupdate(w, omega, hits, up);
+    const int track_links = kPostW ? 0 : track;
     // the links are read again from shared memory below: keep the compiler from
     // holding the values loaded for w(x) in registers across the update instead
     asm volatile("" ::: "memory");
@@ -756,28 +789,32 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
 #pragma unroll 1
         for (int d = 0; d < 3; d++) {
             const uint32_t b = d == 0 ? ib[0] : (d == 1 ? ib[1] : ib[2]);
-            apply_staged<S, true>(my + (2 * d) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, par, i), l.vh, up, track,
-                                  cc);
+            apply_staged<S, true>(my + (2 * d) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, par, i), l.vh, up,
+                                  track_links, cc);
             apply_staged<S, false>(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, op, b), l.vh, up,
-                                   track, cc);
+                                   track_links, cc);
         }
     } else
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         if (d < ND) {
-            apply_staged<S, true>(my + (2 * d) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, par, i), l.vh, up, track,
-                                  cc);
+            apply_staged<S, true>(my + (2 * d) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, par, i), l.vh, up,
+                                  track_links, cc);
             apply_staged<S, false>(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, op, ib[d]), l.vh,
-                                   up, track, cc);
+                                   up, track_links, cc);
         } else {
-            apply_forward<S>(u + su_idx<S>(l, d, par, i), l.vh, up, track, cc);
-            apply_backward<S>(u + su_idx<S>(l, d, op, ib[d]), l.vh, up, track, cc);
+            apply_forward<S>(u + su_idx<S>(l, d, par, i), l.vh, up, track_links, cc);
+            apply_backward<S>(u + su_idx<S>(l, d, op, ib[d]), l.vh, up, track_links, cc);
         }
     }
     if (track) {
-        cc[7] *= 0.57735026918962576451;
+        if constexpr (kPostW) {
+            post = e2_after(up, w0);
+        } else {
+            cc[7] *= 0.57735026918962576451;
 #pragma unroll
-        for (int k = 0; k < 8; k++) post += cc[k] * cc[k];
+            for (int k = 0; k < 8; k++) post += cc[k] * cc[k];
+        }
     }
 }
 
