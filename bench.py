@@ -233,12 +233,16 @@ def run_gfc(a, rk):
 
     # ---- end to end through the C ABI with host buffers: every step uploads its
     # links (raw big-endian bytes) from pinned host memory and reads its G back.  Two
-    # contexts alternate, so the next step's upload, layout and reunitarisation run on
-    # that context's own streams while this step's fix runs (the copy engine and the
-    # SMs work at the same time); every step's transfers are inside the timed region.
+    # contexts alternate, so the next step's upload, layout and reunitarisation, and
+    # the previous step's G download, run on those contexts' own streams while this
+    # step's fix runs (the copy engines and the SMs work at the same time); every
+    # step's transfers are inside the timed region, which ends when the last G has
+    # landed in host memory.
     lat2 = gfc.Lattice(ns, nt, device=rk.local)
     lat2.set_shapes(*lat.shapes())
     ctxs = (lat, lat2)
+    gt_host2 = gfc.PinnedBuffer(V * 144)
+    gt_out = (gt_host.view(np.float64), gt_host2.view(np.float64))
 
     def issue(ctx):   # byte swap, layout and reunitarisation in one pass on the GPU
         ctx.upload_links_reunit(raw.array, 8, byteswap=True)
@@ -256,14 +260,17 @@ def run_gfc(a, rk):
             rc, rep = x.fix(params, fast)
             if rc < 0:
                 raise RuntimeError(f"fix did not converge: rc={rc}")
-            x.download_gt(8, False, out=gt_host.view(np.float64))
+            x.download_gt_async(gt_out[k % 2])
             swept += rep.sweeps
+        lat.sync()
+        lat2.sync()
         return time.perf_counter() - t0, swept
 
     e2e_run(max(a.warmup, 2))
     t_e2e, swept = e2e_run(a.steps)
     e2e_time, e2e_updates, _ = rk.aggregate(t_e2e, swept * half)
     lat2.close()
+    gt_host2.close()
     lat.restore_links()
 
     extras = {}

@@ -217,10 +217,11 @@ static int upload_chunked(gfc_ctx *c, const void *host, size_t bytes_per_slice, 
 }
 
 template <typename F>
-static int download_chunked(gfc_ctx *c, void *host, size_t bytes_per_slice, F fn) {
+static int download_chunked(gfc_ctx *c, void *host, size_t bytes_per_slice, F fn, int wait = 1) {
     const Lat &l = c->lat;
     uint32_t per = (uint32_t)std::max<size_t>(1, c->stage_bytes / bytes_per_slice);
     const int pinned = is_pinned(host);
+    if (!wait && !pinned) return GFC_ERR_ARG;   // an unfinished copy must land in page-locked memory
     int k = 0;
     uint32_t pend_t0[2] = {0, 0}, pend_n[2] = {0, 0};
     int pend[2] = {0, 0};
@@ -247,6 +248,10 @@ static int download_chunked(gfc_ctx *c, void *host, size_t bytes_per_slice, F fn
             pend_t0[k] = t0;
             pend_n[k] = nts;
         }
+    }
+    if (!wait) {
+        GFC_CHECK(cudaGetLastError());
+        return GFC_OK;
     }
     GFC_CHECK(cudaStreamSynchronize(c->sc));
     for (int j = 0; j < 2; j++)
@@ -301,6 +306,23 @@ extern "C" int gfc_ctx_download_gt(gfc_ctx *c, void *host, int elem_bytes, int b
     return download_chunked(c, host, per_slice, [&](void *d, uint32_t t0, uint32_t nts) {
         launch_store_gt(c->g, l, t0, nts, elem_bytes, byteswap, d, c->s);
     });
+}
+
+// The same as gfc_ctx_download_gt, left in flight on the context's streams: the
+// host buffer must be page-locked; gfc_ctx_sync completes it.
+extern "C" int gfc_ctx_download_gt_async(gfc_ctx *c, void *host, int elem_bytes, int byteswap) {
+    if (!c || !host || (elem_bytes != 8 && elem_bytes != 4)) return GFC_ERR_ARG;
+    if (!is_pinned(host)) {
+        set_error("gfc_ctx_download_gt_async: the host buffer is not page-locked");
+        return GFC_ERR_ARG;
+    }
+    GFC_CHECK(cudaSetDevice(c->dev));
+    const Lat l = c->lat;
+    size_t per_slice = (size_t)l.vs * 18 * elem_bytes;
+    return download_chunked(
+        c, host, per_slice,
+        [&](void *d, uint32_t t0, uint32_t nts) { launch_store_gt(c->g, l, t0, nts, elem_bytes, byteswap, d, c->s); },
+        0);
 }
 
 extern "C" int gfc_ctx_download_links(gfc_ctx *c, void *host, int elem_bytes, int byteswap) {
@@ -523,6 +545,7 @@ extern "C" int gfc_ctx_sync(gfc_ctx *c) {
     if (!c) return GFC_ERR_ARG;
     GFC_CHECK(cudaSetDevice(c->dev));
     GFC_CHECK(cudaStreamSynchronize(c->s));
+    GFC_CHECK(cudaStreamSynchronize(c->sc));   // copies left in flight (gfc_ctx_download_gt_async)
     return GFC_OK;
 }
 

@@ -109,6 +109,7 @@ def _load():
         "gfc_ctx_download_links": (I, [P, P, I, I]),
         "gfc_ctx_upload_gt": (I, [P, P, I, I]),
         "gfc_ctx_download_gt": (I, [P, P, I, I]),
+        "gfc_ctx_download_gt_async": (I, [P, P, I, I]),
         "gfc_ctx_get_link": (I, [P, S, I, DP]),
         "gfc_ctx_reunitarize": (I, [P]),
         "gfc_ctx_reunitarize_gt": (I, [P]),
@@ -256,6 +257,13 @@ class Lattice:
         dt = np.float64 if elem_bytes == 8 else np.float32
         out = np.empty(self.V * 18, dtype=dt) if out is None else out
         _check(lib.gfc_ctx_download_gt(self.h, out.ctypes.data, elem_bytes, int(byteswap)), "download_gt")
+        return out
+
+    def download_gt_async(self, out, elem_bytes=8, byteswap=False):
+        """Queue the download of G into `out` (page-locked, e.g. a PinnedBuffer view)
+        and return at once; sync() completes it."""
+        _check(lib.gfc_ctx_download_gt_async(self.h, out.ctypes.data, elem_bytes, int(byteswap)),
+               "download_gt_async")
         return out
 
     def get_link(self, site, mu):

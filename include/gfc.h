@@ -152,7 +152,7 @@ int  gfc_ctx_create(int ns, int nt, int device, int flags, gfc_ctx **out);
 int  gfc_ctx_destroy(gfc_ctx *c);
 long long gfc_ctx_kernel_launches(const gfc_ctx *c);
 void *gfc_ctx_stream(gfc_ctx *c);   /* the context's cudaStream_t, as void* */
-int  gfc_ctx_sync(gfc_ctx *c);
+int  gfc_ctx_sync(gfc_ctx *c);   /* waits for all work and copies queued on the context */
 
 /* Links in, as raw file bytes in the reference order: elem_bytes 8 (FP64) or 4
  * (FP32, converted to FP64 like CONV_CFG_TO_WORKING_PRECISION), byteswap 1 for
@@ -165,6 +165,12 @@ int  gfc_ctx_upload_links_reunit(gfc_ctx *c, const void *host, int elem_bytes, i
 int  gfc_ctx_download_links(gfc_ctx *c, void *host, int elem_bytes, int byteswap);
 int  gfc_ctx_upload_gt(gfc_ctx *c, const void *host, int elem_bytes, int byteswap);
 int  gfc_ctx_download_gt(gfc_ctx *c, void *host, int elem_bytes, int byteswap);
+/* gfc_ctx_download_gt left in flight on the context's streams, so that a pipeline
+ * can read one lattice's G while another context fixes the next: host must be
+ * page-locked (gfc_host_alloc), else GFC_ERR_ARG; gfc_ctx_sync completes it, and
+ * later calls on the context are ordered after it.  No counterpart in the reference
+ * (writeGaugeTransf, fields_io.c:493-565, writes synchronously). */
+int  gfc_ctx_download_gt_async(gfc_ctx *c, void *host, int elem_bytes, int byteswap);
 
 /* one link (mu = 0 temporal, 1..3 z,y,x) at lexicographic site L, 18 doubles
  * (getLink, fields.c:233-271) */

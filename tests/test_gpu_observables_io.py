@@ -173,3 +173,32 @@ def test_fused_upload_and_reunitarise(elem_bytes, swap):
         a.reunitarize()
         b.upload_links_reunit(raw, elem_bytes, swap)
         assert a.download_links().tobytes() == b.download_links().tobytes()
+
+
+@pytest.mark.parametrize("elem_bytes,swap", [(8, False), (4, True)])
+def test_async_gt_download_matches_the_synchronous_one(elem_bytes, swap):
+    """G downloaded with the copy left in flight equals the synchronous download
+    bytewise once the context is synchronised; two downloads in a row into two
+    buffers, with a fix queued in between, each hold the G of their moment;
+    pageable memory is refused."""
+    ns, nt = 6, 5
+    V = ns ** 3 * nt
+    dt = np.float64 if elem_bytes == 8 else np.float32
+    with gfc.Lattice(ns, nt) as lat:
+        lat.upload_links(gfc.synth_config(ns, nt, 171, 0.5), 8, False)
+        lat.set_identity_gt()
+        lat.halfsweeps(0, 7, 1.95, 2)
+        G1 = lat.download_gt(elem_bytes, swap)
+        b1, b2 = gfc.PinnedBuffer(V * 18 * elem_bytes), gfc.PinnedBuffer(V * 18 * elem_bytes)
+        lat.download_gt_async(b1.view(dt), elem_bytes, swap)
+        lat.halfsweeps(7, 5, 1.95, 2)
+        lat.download_gt_async(b2.view(dt), elem_bytes, swap)
+        lat.sync()
+        G2 = lat.download_gt(elem_bytes, swap)
+        assert b1.view(dt).tobytes() == G1.tobytes()
+        assert b2.view(dt).tobytes() == G2.tobytes()
+        assert G1.tobytes() != G2.tobytes()
+        with pytest.raises(gfc.GFCError):
+            lat.download_gt_async(np.empty(V * 18, dtype=dt), elem_bytes, swap)
+        b1.close()
+        b2.close()
