@@ -872,15 +872,8 @@ static void launch_bsweep_k(int grid, cudaStream_t st, const BState &bs) {
     constexpr size_t bytes = STG ? (size_t)6 * S::NS * BCHUNK * 16 : 0;
     auto kern = k_bsweep<S, MINB, STG>;
     if constexpr (STG) {
-        static unsigned long long done = 0;   // attribute set once per device
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev < 64 && !(done >> dev & 1ull)) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared);
-            done |= 1ull << dev;
-        }
+        static std::atomic<unsigned long long> done{0};
+        smem_attr_once(done, kern, bytes);
     }
     kern<<<grid, BCHUNK, bytes, st>>>(bs);
 }

@@ -372,15 +372,8 @@ static void launch_staged(dim3 grid, cudaStream_t st, typename S::V *u, typename
     static_assert(bytes <= 227 * 1024, "staged tile exceeds shared memory");
     static_assert(sh.block >= MIN_BLOCK, "block partial buffers are sized for MIN_BLOCK");
     auto kern = k_sweep_staged<S, sh.block, sh.minb, (bool)sh.sg, sh.nst>;
-    // the attribute is set once per device (a CUDA function attribute is per context)
-    static unsigned long long done = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 64 && !(done >> dev & 1ull)) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-        done |= 1ull << dev;
-    }
+    static std::atomic<unsigned long long> done{0};
+    smem_attr_once(done, kern, bytes);
     grid.x = ((a.l.vs >> 1) + sh.block - 1) / sh.block;
     kern<<<grid, sh.block, bytes, st>>>(u, g, a);
 }

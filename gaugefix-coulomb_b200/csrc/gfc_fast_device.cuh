@@ -34,11 +34,11 @@ __device__ __forceinline__ C mkc(decltype(C::x) a, decltype(C::x) b) {
 }
 template <typename C>
 __device__ __forceinline__ C fmul(C a, C b) {
-    return mkc<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return mkc<C>(fma(a.x, b.x, -(a.y * b.y)), fma(a.x, b.y, a.y * b.x));
 }
 template <typename C>
 __device__ __forceinline__ C fmul_conj(C a, C b) {  // a * conj(b)
-    return mkc<C>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+    return mkc<C>(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -(a.x * b.y)));
 }
 template <typename C>
 __device__ __forceinline__ C fadd(C a, C b) {
@@ -49,7 +49,10 @@ __device__ __forceinline__ C fconj(C a) {
     return mkc<C>(a.x, -a.y);
 }
 // s + a b, s + a conj(b) and s - a b as chains of fused multiply-adds (four per
-// complex product instead of two products, two fused operations and two sums)
+// complex product instead of two products, two fused operations and two sums).
+// Every multiply-add of the fast update is written out as fma(): the compiler is
+// left no choice of which products to fuse, so each launch shape of one kernel body
+// computes the same bits.
 template <typename C>
 __device__ __forceinline__ C fmac(C s, C a, C b) {
     return mkc<C>(fma(-a.y, b.y, fma(a.x, b.x, s.x)), fma(a.y, b.x, fma(a.x, b.y, s.y)));
@@ -199,7 +202,14 @@ __device__ __forceinline__ double e2_from_w(const Mt<T> &w) {
     double c6 = (double)w.e[5].y + (double)w.e[7].y;
     double c7 = (double)w.e[5].x - (double)w.e[7].x;
     double c8 = ((double)w.e[0].y + (double)w.e[4].y - 2.0 * (double)w.e[8].y) * 0.57735026918962576451;
-    return c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4 + c5 * c5 + c6 * c6 + c7 * c7 + c8 * c8;
+    double q = c1 * c1;
+    q = fma(c2, c2, q);
+    q = fma(c3, c3, q);
+    q = fma(c4, c4, q);
+    q = fma(c5, c5, q);
+    q = fma(c6, c6, q);
+    q = fma(c7, c7, q);
+    return fma(c8, c8, q);
 }
 
 // e2 density of a site after its update: in a half-sweep the six links of x change
@@ -231,7 +241,7 @@ __device__ __forceinline__ bool fsub_coef(const Mt<T> &w, typename CT<T>::t (&x)
     T k1 = -(w.e[EL(A, B)].y + w.e[EL(B, A)].y);
     T k2 = -(w.e[EL(A, B)].x - w.e[EL(B, A)].x);
     T k3 = -(w.e[EL(A, A)].y - w.e[EL(B, B)].y);
-    T n = k0 * k0 + k1 * k1 + k2 * k2 + k3 * k3;
+    const T n = fma(k3, k3, fma(k2, k2, fma(k1, k1, k0 * k0)));
     if (n == T(0)) return false;
     T r = frsqrt(n);
     k0 *= r;
@@ -290,18 +300,27 @@ __device__ __forceinline__ void fhit_first(Mt<T> &w, Mt<T> &g) {
     g.e[8] = fmul(t[3], s[3]);
 }
 
+// squared norm of a complex 3-vector as one chain of fused multiply-adds
+template <typename C>
+__device__ __forceinline__ decltype(C::x) fnorm2(C a, C b, C c) {
+    decltype(C::x) n = a.x * a.x;
+    n = fma(a.y, a.y, n);
+    n = fma(b.x, b.x, n);
+    n = fma(b.y, b.y, n);
+    n = fma(c.x, c.x, n);
+    return fma(c.y, c.y, n);
+}
+
 template <typename T>
 __device__ __forceinline__ bool fproject(Mt<T> &m) {
     using C = typename CT<T>::t;
-    T n0 = m.e[0].x * m.e[0].x + m.e[0].y * m.e[0].y + m.e[1].x * m.e[1].x + m.e[1].y * m.e[1].y +
-           m.e[2].x * m.e[2].x + m.e[2].y * m.e[2].y;
+    const T n0 = fnorm2(m.e[0], m.e[1], m.e[2]);
     if (n0 == T(0)) return false;
     T r0 = frsqrt(n0);
 #pragma unroll
     for (int k = 0; k < 3; k++) m.e[k] = mkc<C>(m.e[k].x * r0, m.e[k].y * r0);
     fcross_conj(&m.e[0], &m.e[3], &m.e[6]);
-    T n2 = m.e[6].x * m.e[6].x + m.e[6].y * m.e[6].y + m.e[7].x * m.e[7].x + m.e[7].y * m.e[7].y +
-           m.e[8].x * m.e[8].x + m.e[8].y * m.e[8].y;
+    const T n2 = fnorm2(m.e[6], m.e[7], m.e[8]);
     if (n2 == T(0)) return false;
     T r2 = frsqrt(n2);
 #pragma unroll
@@ -342,7 +361,8 @@ __device__ __forceinline__ void fupdate(Mt<T> &w, T omega, unsigned hits, Mt<T> 
 #pragma unroll
         for (int b = 0; b < 3; b++) {
             C x = g.e[EL(a, b)];
-            g.e[EL(a, b)] = a == b ? mkc<C>(T(1) + omega * (x.x - T(1)), omega * x.y) : mkc<C>(omega * x.x, omega * x.y);
+            g.e[EL(a, b)] = a == b ? mkc<C>(fma(omega, x.x - T(1), T(1)), omega * x.y)
+                                   : mkc<C>(omega * x.x, omega * x.y);
         }
     if (!fproject(g)) fidentity(g);
 }

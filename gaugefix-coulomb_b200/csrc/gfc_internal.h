@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "gfc_device.cuh"
 
 // bits of the device status word
@@ -13,6 +15,21 @@
 struct gfc_batch;
 
 namespace gfc {
+
+// Raise a kernel's dynamic shared-memory limit (and prefer shared memory in the
+// L1/shared split) on the current device, once per device: a function attribute
+// belongs to the device's context.  Host threads racing on one device may both set
+// it, which is harmless; the device's bit is set only after the attribute is.
+template <typename K>
+inline void smem_attr_once(std::atomic<unsigned long long> &done, K kern, size_t bytes) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = dev >= 0 && dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (bit) done.fetch_or(bit, std::memory_order_release);
+}
 
 // ---- exact FP64 kernels (gfc_kernels_exact.cu)
 // stop (optional): a device stop word; once set, the launch does nothing

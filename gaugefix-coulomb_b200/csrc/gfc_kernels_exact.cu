@@ -162,14 +162,8 @@ static void launch_exact_staged(const Lat &l, double2 *u, double2 *g, int par, d
     constexpr size_t bytes = (size_t)6 * 9 * BLOCK * sizeof(double2);
     static_assert(bytes <= 227 * 1024, "staged links exceed shared memory");
     auto kern = k_sweep_exact_staged<BLOCK, MINB>;
-    static unsigned long long done = 0;   // attribute set once per device
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 64 && !(done >> dev & 1ull)) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-        done |= 1ull << dev;
-    }
+    static std::atomic<unsigned long long> done{0};
+    smem_attr_once(done, kern, bytes);
     kern<<<(l.vh + BLOCK - 1) / BLOCK, BLOCK, bytes, s>>>(u, g, l, par, omega, hits, stop);
 }
 
