@@ -78,7 +78,7 @@ struct SShape {
     int block, minb, sg, nst;   // nst: links staged per site (whole directions: 2, 4 or 6)
 };
 constexpr SShape kStaged[] = {{128, 2, 1, 6}, {64, 5, 1, 6}, {128, 3, 0, 6}, {64, 6, 0, 6}, {32, 11, 0, 6},
-                              {64, 7, 0, 4}, {128, 4, 0, 4}, {64, 6, 0, 4}, {128, 4, 0, 2}};
+                              {32, 12, 0, 6}, {64, 7, 0, 4}, {128, 4, 0, 4}, {128, 4, 0, 2}};
 constexpr int kNumStaged = sizeof(kStaged) / sizeof(kStaged[0]);
 constexpr int kNumAll = kNumShapes + kNumStaged;   // shape indices: plain, then staged
 constexpr int kNE = 5;   // exact-kernel shapes (gfc_kernels_exact.cu)
@@ -108,11 +108,10 @@ __device__ __forceinline__ void fblock_sum(double (&v)[NQ], double (*sh)[BLOCK /
 }
 
 // Combine block partials: last block of a slice sums the slice, last slice sums
-// all slices, applies the stopping test.  Called by all threads of the block.
+// all slices, applies the stopping test.  Called by all threads of the block; sh and
+// last are shared-memory scratch of the block.
 template <int BLOCK>
-__device__ void fused_reduce(const SweepArgs &a, double pre, double post) {
-    __shared__ double sh[2][BLOCK / 32];
-    __shared__ int last;
+__device__ void fused_reduce(const SweepArgs &a, double pre, double post, double (*sh)[BLOCK / 32], int &last) {
     double v[2] = {pre, post};
     fblock_sum<BLOCK, 2>(v, sh);
     const uint32_t t = a.t0 + blockIdx.y, nbx = gridDim.x, nt = gridDim.y;
@@ -190,7 +189,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_fast(typename S::V *__res
     const bool active = off < vsh;
     double pre = 0.0, post = 0.0;
     if (active) fast_site<S>(u, g, l, a.par, (a.t0 + blockIdx.y) * vsh + off, (T)a.omega, a.hits, a.track, pre, post);
-    if (a.track) fused_reduce<BLOCK>(a, pre, post);
+    __shared__ double sh[2][BLOCK / 32];
+    __shared__ int last;
+    if (a.track) fused_reduce<BLOCK>(a, pre, post, sh, last);
 }
 
 template <class S, int BLOCK, int MINB, bool SG, int NST>
@@ -206,7 +207,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_staged(typename S::V *__r
     if (off < vsh)
         fast_site_staged<S, BLOCK, SG, NST>(u, g, l, a.par, (a.t0 + blockIdx.y) * vsh + off, (T)a.omega, a.hits, a.track,
                                        pre, post, (typename S::V *)staged_smem);
-    if (a.track) fused_reduce<BLOCK>(a, pre, post);
+    if (a.track) {
+        // the reduction's scratch reuses the staging buffer: it has no static shared
+        // memory, so 32-site blocks fit 12 to an SM; every thread is done with its
+        // staged links after the barrier
+        __syncthreads();
+        auto *sh = reinterpret_cast<double(*)[BLOCK / 32]>(staged_smem);
+        int &last = *reinterpret_cast<int *>(staged_smem + 2 * (BLOCK / 32) * sizeof(double));
+        fused_reduce<BLOCK>(a, pre, post, sh, last);
+    }
 }
 
 // projectSU3 on entries [begin, begin + count) of each of nblk SoA blocks

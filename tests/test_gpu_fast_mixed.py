@@ -88,7 +88,7 @@ def test_fast_tracks_exact_per_sweep():
 
 # shape indices by kernel body: plain, all six links staged in shared memory, four
 # staged, two staged (gfc_ctx_autotune's order)
-BODIES = [range(0, 9), range(9, 14), range(14, 17), range(17, 18)]
+BODIES = [range(0, 9), range(9, 15), range(15, 17), range(17, 18)]
 
 
 def test_every_launch_shape_gives_the_same_fix():
