@@ -593,7 +593,8 @@ def main():
     cfg = {"workload": f"{a.ns}^3x{a.nt} SU(3) Coulomb gauge fix to e2<={a.tol:g}, omega 1.95, hits 2",
            "lattice": [a.ns, a.nt], "seed": a.seed, "h_scale": a.scale, "tolerance": a.tol,
            "parallelism": f"replicas x{rk.world}" if rk.world > 1 else "1 GPU",
-           "l2": "inputs larger than L2 (1.2 GB of links per replica)"}
+           "l2": (f"inputs larger than L2 ({a.ns ** 3 * a.nt * 4 * 144 / 1e9:.1f} GB of links per replica)"
+                  if a.ns ** 3 * a.nt * 4 * 144 > 126e6 else "inputs smaller than L2, not flushed")}
     if a.impl == "reference":
         if rk.rank == 0:
             r = cpu_reference(a, a.steps, a.warmup, a.cpu_half_sweeps)
