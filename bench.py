@@ -559,15 +559,31 @@ def ref_harness():
     return None
 
 
+def oracle_synth_config(ns, nt, seed, scale):
+    """The workload's input links made by the oracle's restatement of the seeded
+    generator (oracle/liboracle.so; same bytes as the product's generator), so that
+    the reference arm loads no product library."""
+    import ctypes
+
+    import numpy as np
+
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    lib.orc_synth_config.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, ctypes.c_double,
+                                     ctypes.c_void_p]
+    lib.orc_synth_config.restype = ctypes.c_int
+    U = np.empty(ns ** 3 * nt * 4 * 18)
+    if lib.orc_synth_config(ns, nt, seed, scale, U.ctypes.data) != 0:
+        raise MemoryError("orc_synth_config")
+    return U
+
+
 def cpu_reference(a, steps, warmup, half_sweeps):
     """The reference's own half-sweep loop (OpenMP over timeslices) on this host."""
-    import gfc
-
     exe = ref_harness()
-    if exe is None:
+    if exe is None or not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
         return None
     ns, nt = a.ns, a.nt
-    U0 = gfc.synth_config(ns, nt, a.seed, a.scale)
+    U0 = oracle_synth_config(ns, nt, a.seed, a.scale)
     with tempfile.TemporaryDirectory() as d:
         cfg = os.path.join(d, "cfg.be")
         U0.astype(">f8").tofile(cfg)

@@ -544,3 +544,160 @@ int orc_fix(double *Ud, double *Gd, int ns, int nt, double tol, int proxy_theta,
 #undef PROXY
     return rc == 0 ? sweep : rc;
 }
+
+/* ------------------------------------------------------ workload generator --- */
+/*
+ * The seeded synthetic configurations of the benchmark workloads, restated here so
+ * that the reference arm of the benchmark and the fixture script can make their
+ * input files without loading the product library:
+ *
+ *   U_mu(x) = g(x) exp(i s H_mu(x)) g(x + mu)^dagger,  H = sum_a c_a lambda_a / 2,
+ *   c_a ~ N(0, 1), g Haar-random SU(3),
+ *
+ * written big-endian or native by the caller.  Random numbers: one SplitMix64
+ * stream (Steele, Lea, Flood 2014) per (seed, site, slot), slots 0..3 for H_mu and
+ * 4 for g; normal deviates by Box-Muller (cosine first, sine kept for the next
+ * draw).  Haar SU(3) from two complex Gaussian rows by Gram-Schmidt, the third row
+ * conj(r0 x r1); the exponential by a degree-14 Horner Taylor series after scaling
+ * below norm 1/4, then squaring.  Every sum starts from 0 and runs in index order,
+ * FP contraction is off: the bytes must equal the product generator's for the same
+ * arguments, which tests/test_oracle_golden.py pins with the fixtures' sha256.
+ */
+typedef struct { unsigned long long key, n; int spare_ok; double spare; } rng_t;
+
+static inline unsigned long long mix64(unsigned long long z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+#define WEYL 0x9E3779B97F4A7C15ULL
+
+static rng_t rng_for(unsigned long long seed, size_t site, unsigned slot) {
+    rng_t r;
+    r.key = mix64(mix64(seed + WEYL) + ((unsigned long long)site * 8u + slot + 1u) * 0xD1B54A32D192ED03ULL);
+    r.n = 0;
+    r.spare_ok = 0;
+    r.spare = 0.0;
+    return r;
+}
+static double rng_open01(rng_t *r) {
+    r->n += 1;
+    unsigned long long z = mix64(r->key + r->n * WEYL);
+    return ((double)(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+static double rng_gauss(rng_t *r) {
+    if (r->spare_ok) { r->spare_ok = 0; return r->spare; }
+    double a = rng_open01(r), b = rng_open01(r);
+    double rad = sqrt(-2.0 * log(a)), ang = 6.283185307179586476925286766559 * b;
+    r->spare = rad * sin(ang);
+    r->spare_ok = 1;
+    return rad * cos(ang);
+}
+
+static void gen_mul(const mat *a, const mat *b, mat *c, int dag_b) {
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            cplx s = cmk(0.0, 0.0);
+            for (int k = 0; k < 3; k++)
+                s = cadd(s, cmul(a->m[E(i, k)], dag_b ? cconj(b->m[E(j, k)]) : b->m[E(k, j)]));
+            c->m[E(i, j)] = s;
+        }
+}
+
+static void gen_haar(rng_t *r, mat *g) {
+    cplx row[2][3];
+    for (int i = 0; i < 2; i++)
+        for (int c = 0; c < 3; c++) {
+            double re = rng_gauss(r);
+            row[i][c] = cmk(re, rng_gauss(r));
+        }
+    double n = 0.0;
+    for (int c = 0; c < 3; c++) { n += row[0][c].re * row[0][c].re; n += row[0][c].im * row[0][c].im; }
+    n = 1.0 / sqrt(n);
+    for (int c = 0; c < 3; c++) row[0][c] = cmk(row[0][c].re * n, row[0][c].im * n);
+    cplx ip = cmk(0.0, 0.0);                 /* <row0, row1> */
+    for (int c = 0; c < 3; c++) ip = cadd(ip, cmul(cconj(row[0][c]), row[1][c]));
+    for (int c = 0; c < 3; c++) row[1][c] = csub(row[1][c], cmul(ip, row[0][c]));
+    n = 0.0;
+    for (int c = 0; c < 3; c++) { n += row[1][c].re * row[1][c].re; n += row[1][c].im * row[1][c].im; }
+    n = 1.0 / sqrt(n);
+    for (int c = 0; c < 3; c++) row[1][c] = cmk(row[1][c].re * n, row[1][c].im * n);
+    for (int c = 0; c < 3; c++) {
+        g->m[E(0, c)] = row[0][c];
+        g->m[E(1, c)] = row[1][c];
+    }
+    for (int c = 0; c < 3; c++) {
+        int a = (c + 1) % 3, b = (c + 2) % 3;
+        g->m[E(2, c)] = cconj(csub(cmul(row[0][a], row[1][b]), cmul(row[0][b], row[1][a])));
+    }
+}
+
+static void gen_exp(rng_t *r, double s, mat *e) {
+    double c[9];
+    for (int a = 1; a <= 8; a++) c[a] = rng_gauss(r);
+    const double k3 = 1.0 / sqrt(3.0);
+    mat h;
+    memset(&h, 0, sizeof h);
+    h.m[E(0, 0)].re = 0.5 * (c[3] + c[8] * k3);
+    h.m[E(1, 1)].re = 0.5 * (-c[3] + c[8] * k3);
+    h.m[E(2, 2)].re = 0.5 * (-2.0 * c[8] * k3);
+    h.m[E(0, 1)] = cmk(0.5 * c[1], -0.5 * c[2]);
+    h.m[E(1, 0)] = cmk(0.5 * c[1], 0.5 * c[2]);
+    h.m[E(0, 2)] = cmk(0.5 * c[4], -0.5 * c[5]);
+    h.m[E(2, 0)] = cmk(0.5 * c[4], 0.5 * c[5]);
+    h.m[E(1, 2)] = cmk(0.5 * c[6], -0.5 * c[7]);
+    h.m[E(2, 1)] = cmk(0.5 * c[6], 0.5 * c[7]);
+    mat x;                                   /* i s H */
+    double nn = 0.0;
+    for (int k = 0; k < 9; k++) {
+        x.m[k] = cmk(-s * h.m[k].im, s * h.m[k].re);
+        nn += h.m[k].re * h.m[k].re + h.m[k].im * h.m[k].im;
+    }
+    nn = fabs(s) * sqrt(nn);
+    double f = 1.0;
+    int squarings = 0;
+    while (nn * f > 0.25) { f *= 0.5; squarings++; }
+    for (int k = 0; k < 9; k++) x.m[k] = cmk(x.m[k].re * f, x.m[k].im * f);
+    mat acc, t;
+    set_identity(&acc);
+    for (int n = 14; n >= 1; n--) {
+        gen_mul(&x, &acc, &t, 0);
+        for (int k = 0; k < 9; k++) acc.m[k] = cmk(t.m[k].re / (double)n, t.m[k].im / (double)n);
+        for (int i = 0; i < 3; i++) acc.m[E(i, i)].re += 1.0;
+    }
+    for (int k = 0; k < squarings; k++) {
+        gen_mul(&acc, &acc, &t, 0);
+        acc = t;
+    }
+    *e = acc;
+}
+
+/* U: 4 V matrices in the reference's order, native doubles.  Returns 0, or -1. */
+int orc_synth_config(int ns, int nt, unsigned long long seed, double scale, double *Ud) {
+    if (ns <= 0 || nt <= 0 || !Ud) return -1;
+    geo geom = {ns, nt};
+    const size_t V = (size_t)ns * ns * ns * nt;
+    mat *g = malloc(V * sizeof(mat));
+    if (!g) return -1;
+    #pragma omp parallel for schedule(static)
+    for (long long L = 0; L < (long long)V; L++) {
+        rng_t r = rng_for(seed, (size_t)L, 4);
+        gen_haar(&r, &g[L]);
+    }
+    #pragma omp parallel for schedule(static)
+    for (long long L = 0; L < (long long)V; L++) {
+        int p[4] = {(int)(L / ((long long)ns * ns * ns)), (int)((L / ((long long)ns * ns)) % ns),
+                    (int)((L / ns) % ns), (int)(L % ns)};
+        for (int mu = 0; mu < 4; mu++) {
+            int q[4];
+            neighbour(&geom, p, mu, +1, q);
+            rng_t r = rng_for(seed, (size_t)L, (unsigned)mu);
+            mat e, ge;
+            gen_exp(&r, scale, &e);
+            gen_mul(&g[L], &e, &ge, 0);
+            gen_mul(&ge, &g[site_pos(&geom, q)], (mat *)Ud + (size_t)L * 4 + mu, 1);
+        }
+    }
+    free(g);
+    return 0;
+}

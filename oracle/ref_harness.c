@@ -8,12 +8,16 @@
  * reference is copied here; this file only calls it.
  *
  * Modes:
- *   trace <cfg> <ns> <nt> <params|-> <out_prefix> [max_trace]
+ *   trace <cfg> <ns> <nt> <params|-> <out_prefix> [max_trace] [trace_every] [dump_sweep]
  *       loadConfig + reunitarizeField + the gaugefixOverrelaxation loop
  *       (gauge_fixing.c:749-826) re-driven half-sweep by half-sweep, recording
- *       calculate_e2 and calculateF after every half-sweep.  Writes
- *       <out_prefix>.trace (text: sweep e2 F), <out_prefix>.gt (final G, native
- *       doubles), <out_prefix>.u (final U) and <out_prefix>.summary.
+ *       calculate_e2 and calculateF after every half-sweep up to max_trace and
+ *       after every trace_every-th half-sweep beyond it (large lattices: the
+ *       reference's e2 and F are serial loops).  Writes <out_prefix>.trace (text:
+ *       sweep e2 F), <out_prefix>.gt (final G, native doubles), <out_prefix>.u
+ *       (final U), <out_prefix>.summary and, when the loop passes dump_sweep,
+ *       <out_prefix>.gt_dump (G right after that half-sweep and the reunitarisation
+ *       that follows it, if one is due).
  *   bench <cfg> <ns> <nt> <half_sweeps> [threads]
  *       times <half_sweeps> half-sweeps of the reference loop body (OpenMP over t,
  *       as gauge_fixing.c:773-787) with omp_get_wtime and prints one line:
@@ -91,12 +95,16 @@ int main(int argc, char **argv) {
                                                       : initParametersORDefault();
     const char *prefix = argv[6];
     int max_trace = argc > 7 ? atoi(argv[7]) : 100000;
+    int trace_every = argc > 8 ? atoi(argv[8]) : 0;
+    int dump_sweep = argc > 9 ? atoi(argv[9]) : -1;
     char path[1024];
     snprintf(path, sizeof path, "%s.trace", prefix);
     FILE *tr = fopen(path, "w");
     if (!tr) return 5;
 
     setFieldToIdentity(G, V);
+    const double plaq_s0 = (double)averagePlaquette(U, "spatial");
+    const double plaq_t0 = (double)averagePlaquette(U, "temporal");
     int sweep = 0, rc = 0;
     double res = p.generic_gf.gfix_proxy(U);
     fprintf(tr, "%d %.17e %.17e\n", 0, calculate_e2(U), calculateF(U));
@@ -112,7 +120,10 @@ int main(int argc, char **argv) {
             }
         }
         sweep++;
-        if (sweep <= max_trace) fprintf(tr, "%d %.17e %.17e\n", sweep, calculate_e2(U), calculateF(U));
+        if (sweep <= max_trace || (trace_every > 0 && sweep % trace_every == 0)) {
+            fprintf(tr, "%d %.17e %.17e\n", sweep, calculate_e2(U), calculateF(U));
+            fflush(tr);
+        }
         if (sweep == due) {
             double last = res;
             res = p.generic_gf.gfix_proxy(U);
@@ -124,6 +135,10 @@ int main(int argc, char **argv) {
         if (!(sweep % p.generic_gf.sweeps_to_reunitarization)) {
             reunitarizeField(U, DIM * V);
             reunitarizeField(G, V);
+        }
+        if (sweep == dump_sweep) {
+            snprintf(path, sizeof path, "%s.gt_dump", prefix);
+            write_doubles(path, G, (size_t)V * 18);
         }
     }
     if (rc == 0) {
@@ -138,9 +153,10 @@ int main(int argc, char **argv) {
     snprintf(path, sizeof path, "%s.summary", prefix);
     FILE *s = fopen(path, "w");
     fprintf(s, "sweeps %d\nrc %d\nfinal_residue %.17e\ne2 %.17e\ntheta %.17e\nF %.17e\n"
-               "plaq_spatial %.17e\nplaq_temporal %.17e\n",
+               "plaq_spatial %.17e\nplaq_temporal %.17e\nplaq_spatial_0 %.17e\nplaq_temporal_0 %.17e\n",
             rc == 0 ? sweep : rc, rc, p.generic_gf.gfix_proxy(U), calculate_e2(U), calculateTheta(U),
-            calculateF(U), (double)averagePlaquette(U, "spatial"), (double)averagePlaquette(U, "temporal"));
+            calculateF(U), (double)averagePlaquette(U, "spatial"), (double)averagePlaquette(U, "temporal"),
+            plaq_s0, plaq_t0);
     fclose(s);
     return 0;
 }

@@ -10,6 +10,16 @@ seeded synthetic configurations and records, per case:
 
 Needs the reference sources (only in the build container); the fixtures are
 committed so the tests run anywhere.  Usage:  python tests/golden/make_golden.py
+
+  --full   instead runs the reference's complete fix of the two full-size workloads
+           (32^3x64 FP64, seed 2, H 0.5; 48^3x96 stored FP32, seed 3, H 0.7; tolerance
+           1e-15) through oracle/_ref/ref_harness (ref_harness_f32in for FP32 files)
+           and writes full_cases.json (sweep count, return code, final residue, e2, F,
+           theta, plaquettes before and after, sha256 of G and of the spatial links),
+           <name>_trace.npy (e2 and F after the first 20 half-sweeps and after every
+           50th) and <name>_gt_sample.npy (G at every sample_stride-th site, after
+           half-sweep dump_sweep and at the end).  About 10 min (32^3x64) and 40 min
+           (48^3x96) on 8 host cores.
 """
 import hashlib
 import json
@@ -23,8 +33,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-sys.path.insert(0, os.path.join(ROOT, "gaugefix-coulomb_b200"))
-import gfc  # noqa: E402  (host-only functions: the generator)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+import oracle_ref as orc  # noqa: E402  (the oracle's restatement of the workload generator)
 
 REF = os.path.join(ROOT, "oracle", "_ref")
 
@@ -59,7 +69,7 @@ def write_params(path, kv):
 
 
 def config_bytes(ns, nt, seed, scale, in_bytes):
-    U = gfc.synth_config(ns, nt, seed, scale)
+    U = orc.synth_config(ns, nt, seed, scale)
     return U.astype(">f8" if in_bytes == 8 else ">f4").tobytes()
 
 
@@ -158,7 +168,66 @@ def param_file_cases(tmp):
     return out
 
 
+# name, ns, nt, seed, scale, in_bytes, params, dense trace length, trace stride, dump sweep, sample stride
+FULL_CASES = [
+    ("cfg1_32x64", 32, 64, 2, 0.5, 8, dict(tolerance="1.0E-15"), 20, 50, 700, 2039),
+    ("cfg2_48x96_f32in", 48, 96, 3, 0.7, 4, dict(tolerance="1.0E-15"), 20, 50, 700, 10337),
+]
+
+
+def run_full_case(name, ns, nt, seed, scale, in_bytes, params, dense, every, dump, stride, tmp):
+    import time
+    rec = dict(name=name, ns=ns, nt=nt, seed=seed, scale=scale, in_bytes=in_bytes, params=params,
+               dump_sweep=dump, sample_stride=stride)
+    raw = config_bytes(ns, nt, seed, scale, in_bytes)
+    rec["cfg_sha256"] = sha(raw)
+    cfg = os.path.join(tmp, f"{name}.cfg")
+    with open(cfg, "wb") as f:
+        f.write(raw)
+    del raw
+    par = os.path.join(tmp, f"{name}.par")
+    write_params(par, params)
+    V = ns ** 3 * nt
+    prefix = os.path.join(tmp, name)
+    prog = "ref_harness" if in_bytes == 8 else "ref_harness_f32in"
+    t0 = time.time()
+    subprocess.run([os.path.join(REF, prog), "trace", cfg, str(ns), str(nt), par, prefix, str(dense), str(every),
+                    str(dump)], check=True, capture_output=True, cwd=tmp)
+    rec["reference_seconds"] = round(time.time() - t0, 1)
+    for line in open(prefix + ".summary"):
+        k, v = line.split()
+        rec[k] = float(v) if "." in v or "e" in v else int(v)
+    gt = np.fromfile(prefix + ".gt", dtype=np.float64)
+    rec["gt_sha256"] = sha(gt.tobytes())
+    u = np.fromfile(prefix + ".u", dtype=np.float64).reshape(V, 4, 18)
+    rec["u_spatial_sha256"] = sha(np.ascontiguousarray(u[:, 1:4, :]).tobytes())
+    del u
+    gd = np.fromfile(prefix + ".gt_dump", dtype=np.float64)
+    sites = np.arange(0, V, stride)
+    sample = np.stack([gd.reshape(V, 18)[sites], gt.reshape(V, 18)[sites]])
+    np.save(os.path.join(HERE, f"{name}_gt_sample.npy"), sample)
+    np.save(os.path.join(HERE, f"{name}_trace.npy"), np.loadtxt(prefix + ".trace"))
+    for ext in (".gt", ".gt_dump", ".u", ".cfg"):
+        os.remove(prefix + ext if ext != ".cfg" else cfg)
+    return rec
+
+
+def main_full():
+    if not os.path.exists(os.path.join(REF, "ref_harness_f32in")):
+        sys.exit("oracle/_ref is not built (make -C oracle REF=<reference tree>)")
+    recs = []
+    with tempfile.TemporaryDirectory() as tmp:
+        for c in FULL_CASES:
+            recs.append(run_full_case(*c, tmp=tmp))
+            print(recs[-1]["name"], recs[-1]["sweeps"], recs[-1]["final_residue"], recs[-1]["reference_seconds"],
+                  flush=True)
+            with open(os.path.join(HERE, "full_cases.json"), "w") as f:
+                json.dump(recs, f, indent=1)
+
+
 def main():
+    if "--full" in sys.argv:
+        return main_full()
     if not os.path.exists(os.path.join(REF, "ref_harness")):
         sys.exit("oracle/_ref is not built (make -C oracle with the reference sources present)")
     with tempfile.TemporaryDirectory() as tmp:

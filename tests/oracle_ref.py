@@ -25,6 +25,8 @@ _lib.orc_functional.restype = _D
 _lib.orc_plaquette.argtypes = [_P, _I, _I, _I]
 _lib.orc_plaquette.restype = _D
 _lib.orc_apply_gt.argtypes = [_P, _P, _I, _I]
+_lib.orc_synth_config.argtypes = [_I, _I, ctypes.c_ulonglong, _D, _P]
+_lib.orc_synth_config.restype = _I
 
 
 def sha(a):
@@ -75,6 +77,15 @@ def fix(U, G, ns, nt, tol=1e-16, theta_proxy=False, max_sweeps=100000, estimate=
                       omega, hits, tr.ctypes.data if trace_len else None, ftr.ctypes.data if trace_len else None,
                       trace_len, fr.ctypes.data, 0)
     return rc, fr[0], tr[:trace_len], ftr[:trace_len]
+
+
+def synth_config(ns, nt, seed, scale):
+    """The seeded workload construction restated in the oracle (same bytes as the
+    product's generator for the same arguments)."""
+    U = np.empty(ns ** 3 * nt * 4 * 18)
+    if _lib.orc_synth_config(ns, nt, seed, scale, U.ctypes.data) != 0:
+        raise MemoryError("orc_synth_config")
+    return U
 
 
 def case_params(case):

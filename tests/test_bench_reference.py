@@ -39,3 +39,17 @@ def test_reference_arm_other_ranks_do_no_work():
     p = run({"WORLD_SIZE": "2", "RANK": "1", "LOCAL_RANK": "1"})
     assert p.returncode == 0, p.stderr
     assert p.stdout.strip() == ""
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="the reference harness is not built here")
+def test_reference_arm_loads_no_product_library():
+    """The reference arm makes its input with the oracle's generator: the product
+    library (gaugefix-coulomb_b200/lib/libgfc.so) is never mapped into its process."""
+    code = ("import runpy, sys; sys.argv = %r; runpy.run_path(%r, run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('PRODUCT-LOADED' if 'libgfc' in maps else 'CLEAN', 'oracle' in maps)"
+            % (ARGS[1:], ARGS[1]))
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0")
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
+    assert p.returncode == 0, p.stderr
+    assert p.stdout.strip().splitlines()[-1] == "CLEAN True"
