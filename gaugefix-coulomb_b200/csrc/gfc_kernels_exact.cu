@@ -13,6 +13,8 @@
 //
 // Memory traffic per site-update: 6 links + G read and written = 14 x 144 B.
 #include "gfc_device.cuh"
+#include "gfc.h"
+#include "gfc_ctx.h"
 #include "gfc_internal.h"
 
 namespace gfc {
@@ -459,3 +461,21 @@ void launch_functional(const double2 *u, const Lat &l, double *part, double *out
 }
 
 }  // namespace gfc
+
+// Architecture of the device code the runtime loaded for this library on `device`
+// (cudaFuncGetAttributes of the exact half-sweep kernel): binaryVersion 100 is
+// sm_100a machine code; ptxVersion 0 means no PTX was embedded for JIT.
+extern "C" int gfc_device_code_version(int device, int *binary_version, int *ptx_version) {
+    if (!binary_version || !ptx_version) {
+        gfc::set_error("gfc_device_code_version: null output");
+        return GFC_ERR_ARG;
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return gfc::cuda_fail(e, "gfc_device_code_version: cudaSetDevice");
+    cudaFuncAttributes a;
+    e = cudaFuncGetAttributes(&a, gfc::k_identity);
+    if (e != cudaSuccess) return gfc::cuda_fail(e, "gfc_device_code_version: cudaFuncGetAttributes");
+    *binary_version = a.binaryVersion;
+    *ptx_version = a.ptxVersion;
+    return GFC_OK;
+}

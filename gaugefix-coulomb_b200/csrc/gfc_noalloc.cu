@@ -20,7 +20,13 @@
 //
 // The first call on each device looks up the array's device address
 // (cudaGetSymbolAddress) with that device current and caches it; make that first
-// call before any stream capture.
+// call before any stream capture.  Every call is synchronous: it copies its two
+// sums back to the host and waits for them on `stream` before returning.
+//
+// The links must be device memory of the current device (or managed memory):
+// cudaPointerGetAttributes, which allocates nothing, is asked first, and pageable
+// or page-locked host memory and another GPU's memory are refused before any
+// kernel is launched.
 #include <mutex>
 
 #include "gfc.h"
@@ -202,6 +208,26 @@ extern "C" int gfc_e2_theta_device_noalloc(int ns, int nt, const double *u_dev, 
     if ((uintptr_t)u_dev % 16) {
         set_error("gfc_e2_theta_device_noalloc: u_dev must be 16-byte aligned (complex doubles are read in pairs)");
         return GFC_ERR_ARG;
+    }
+    {
+        int cur = -1;
+        GFC_CHECK(cudaGetDevice(&cur));
+        cudaPointerAttributes pa;
+        const cudaError_t pe = cudaPointerGetAttributes(&pa, u_dev);
+        if (pe != cudaSuccess) {
+            (void)cudaGetLastError();
+            set_error("gfc_e2_theta_device_noalloc: u_dev is not a pointer the CUDA runtime knows (%s)",
+                      cudaGetErrorString(pe));
+            return GFC_ERR_ARG;
+        }
+        const bool ok = pa.type == cudaMemoryTypeManaged || (pa.type == cudaMemoryTypeDevice && pa.device == cur);
+        if (!ok) {
+            set_error("gfc_e2_theta_device_noalloc: u_dev must be device memory of the current device %d "
+                      "(it is %s memory of device %d)", cur,
+                      pa.type == cudaMemoryTypeHost ? "page-locked host"
+                      : pa.type == cudaMemoryTypeDevice ? "device" : "unregistered host", pa.device);
+            return GFC_ERR_ARG;
+        }
     }
     const uint64_t V = (uint64_t)ns * ns * ns * nt;
     if (V * 4 >= (1ull << 31)) {

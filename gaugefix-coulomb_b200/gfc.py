@@ -98,6 +98,7 @@ def _load():
         "gfc_write_all": (I, [ctypes.c_char_p, P, S]),
         "gfc_byteswap": (I, [P, S, S]),
         "gfc_last_error": (ctypes.c_char_p, []),
+        "gfc_device_code_version": (I, [I, ctypes.POINTER(I), ctypes.POINTER(I)]),
         "gfc_host_alloc": (P, [S]),
         "gfc_host_free": (None, [P]),
         "gfc_ctx_create": (I, [I, I, I, I, ctypes.POINTER(P)]),
@@ -174,6 +175,13 @@ def options(**kw):
     for k, v in kw.items():
         setattr(o, k, v)
     return o
+
+
+def device_code_version(device=0):
+    """(binaryVersion, ptxVersion) of the library's kernels as loaded on `device`."""
+    b, p = ctypes.c_int(), ctypes.c_int()
+    _check(lib.gfc_device_code_version(device, ctypes.byref(b), ctypes.byref(p)), "gfc_device_code_version")
+    return b.value, p.value
 
 
 def synth_config(ns, nt, seed, scale):

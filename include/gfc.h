@@ -145,6 +145,10 @@ typedef struct gfc_ctx gfc_ctx;
 #define GFC_CTX_MIXED 1   /* also allocate the FP32 fields and the FP64 copy used by GFC_PREC_MIXED */
 
 const char *gfc_last_error(void);
+/* Architecture of the library's device code as loaded on `device`
+ * (cudaFuncGetAttributes): binary_version 100 = sm_100a machine code, ptx_version 0
+ * = no PTX embedded.  No counterpart in the reference (it has no device code). */
+int  gfc_device_code_version(int device, int *binary_version, int *ptx_version);
 /* page-locked host memory for fast transfers (cudaMallocHost / cudaFreeHost) */
 void *gfc_host_alloc(size_t bytes);
 void  gfc_host_free(void *p);
@@ -238,8 +242,11 @@ int  gfc_ctx_get_blocking(const gfc_ctx *c, int *slices64, int *sweeps64, int *s
  * whose partial sums do not fit are rejected with GFC_ERR_ARG and a message in
  * gfc_last_error().  Calls share that array: calls that overlap on the GPU race.
  * The first call on a device looks up the array's address; make it before any
- * stream capture.  stream is a cudaStream_t (NULL: the legacy default stream);
- * the call waits for its own result. */
+ * stream capture.  stream is a cudaStream_t (NULL: the legacy default stream).
+ * The call is synchronous: it copies e2 and theta to the host and waits for them.
+ * u_dev must be device memory of the current device or managed memory
+ * (cudaPointerGetAttributes is asked first); host memory and another GPU's memory
+ * are refused with GFC_ERR_ARG before any kernel runs. */
 #define GFC_NOALLOC_SCRATCH_DOUBLES 16384
 int  gfc_e2_theta_device_noalloc(int ns, int nt, const double *u_dev, void *stream, double *e2, double *theta);
 

@@ -202,3 +202,11 @@ def test_async_gt_download_matches_the_synchronous_one(elem_bytes, swap):
             lat.download_gt_async(np.empty(V * 18, dtype=dt), elem_bytes, swap)
         b1.close()
         b2.close()
+
+
+def test_device_code_is_sm100a():
+    """The kernels the runtime loaded for this library are sm_100a machine code
+    (cudaFuncGetAttributes through the C ABI), with no PTX left for JIT."""
+    binary, ptx = gfc.device_code_version(0)
+    assert binary == 100, (binary, ptx)
+    assert ptx == 0, (binary, ptx)

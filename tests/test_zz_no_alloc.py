@@ -6,8 +6,9 @@ other work sharing the GPU.  It takes links that already live in device memory
 (the caller's buffer) and keeps its scratch in a fixed array inside the library.
 
 Checked here through the C ABI against the context entry point (gfc_ctx_e2, which
-allocates its own scratch), on two calls in a row so that the second call sees the
-scratch the first one left behind.  This file is collected last on purpose.
+allocates its own scratch) and against the CPU oracle's calculate_e2 and
+calculateTheta, on two calls in a row so that the second call sees the scratch the
+first one left behind.  This file is collected last on purpose.
 """
 import ctypes
 
@@ -15,6 +16,7 @@ import numpy as np
 import pytest
 
 import gfc
+import oracle_ref as orc
 
 pytestmark = pytest.mark.gpu
 
@@ -40,6 +42,8 @@ def test_noalloc_matches_context_entry_point(ns, nt, seed):
         assert rc == gfc.GFC_OK, gfc.last_error()
         assert e2 == pytest.approx(e2_ref, rel=1e-13)
         assert th == pytest.approx(th_ref, rel=1e-13)
+        assert e2 == pytest.approx(orc.e2(U, ns, nt), rel=1e-12)
+        assert th == pytest.approx(orc.theta(U, ns, nt), rel=1e-12)
     # a second, different lattice right after: no stale partial sums are reused
     U2 = gfc.synth_config(4, 5, seed + 100, 0.4)
     with gfc.Lattice(4, 5) as lat:
@@ -50,11 +54,13 @@ def test_noalloc_matches_context_entry_point(ns, nt, seed):
     rc, e2b, thb = noalloc(4, 5, u2_dev.data_ptr(), torch.cuda.current_stream().cuda_stream)
     assert rc == gfc.GFC_OK
     assert e2b == pytest.approx(e2b_ref, rel=1e-13) and thb == pytest.approx(thb_ref, rel=1e-13)
+    assert e2b == pytest.approx(orc.e2(U2, 4, 5), rel=1e-12) and thb == pytest.approx(orc.theta(U2, 4, 5), rel=1e-12)
 
 
 def test_noalloc_rejects_what_does_not_fit():
-    """Too many timeslices for the fixed scratch, or a misaligned pointer: a clear
-    error, no kernel launched (the pointer is never dereferenced)."""
+    """Too many timeslices for the fixed scratch, a misaligned pointer, or links
+    that are not in this GPU's memory: a clear error, no kernel launched (the
+    pointer is never dereferenced)."""
     import torch
 
     buf = torch.zeros(64, dtype=torch.float64, device="cuda:0")
@@ -62,3 +68,8 @@ def test_noalloc_rejects_what_does_not_fit():
     assert rc == -10 and "scratch" in gfc.last_error()
     rc, _, _ = noalloc(2, 2, buf.data_ptr() + 8)
     assert rc == -10 and "aligned" in gfc.last_error()
+    # page-locked host memory is reachable from the GPU, but it is not device memory
+    # of this GPU: refused before any launch
+    host = torch.zeros(2 ** 3 * 2 * 4 * 18, dtype=torch.float64).pin_memory()
+    rc, _, _ = noalloc(2, 2, host.data_ptr())
+    assert rc == -10 and "device memory" in gfc.last_error()
