@@ -508,8 +508,7 @@ extern "C" int gfc_ctx_halfsweeps(gfc_ctx *c, int first_sweep, int n, float omeg
     const double omega = (double)omega_OR;
     if (precision == GFC_PREC_FP64_EXACT || !c->lat.cb) {
         for (int k = 0; k < n; k++) {
-            launch_sweep_exact(c->u, c->g, c->lat, first_sweep + k, omega, hits, c->s, c->shape_exact);
-            c->launches++;
+            c->launches += launch_sweep_exact(c->u, c->g, c->lat, first_sweep + k, omega, hits, c->s, c->shape_exact);
         }
     } else if (n > 0) {
         int rc = halfsweeps_fast64(c, first_sweep, n, omega, hits);
@@ -587,8 +586,7 @@ static int fix_reference_schedule(gfc_ctx *c, const gfc_params *p, const gfc_opt
         n = std::max(n, 1);
         if (o->precision == GFC_PREC_FP64_EXACT || !l.cb) {
             for (int k = 0; k < n; k++) {
-                launch_sweep_exact(c->u, c->g, l, sweep + k, omega, p->hits, c->s, c->shape_exact);
-                c->launches++;
+                c->launches += launch_sweep_exact(c->u, c->g, l, sweep + k, omega, p->hits, c->s, c->shape_exact);
             }
         } else {
             e = halfsweeps_fast64(c, sweep, n, omega, p->hits);
@@ -662,8 +660,7 @@ static int fix_every_sweep_exact(gfc_ctx *c, const gfc_params *p, const gfc_opti
         int end = std::min(max, sweep + 32);
         if (period > 0) end = std::min(end, (sweep / period + 1) * period);
         for (; sweep < end; sweep++) {
-            launch_sweep_exact(c->u, c->g, l, sweep, omega, p->hits, c->s, c->shape_exact, stop);
-            c->launches++;
+            c->launches += launch_sweep_exact(c->u, c->g, l, sweep, omega, p->hits, c->s, c->shape_exact, stop);
             if (dense || sweep + 1 == end) {
                 launch_obs(c->u, l, c->part, c->dres, nullptr, c->s, stop);
                 launch_exact_check(c->dres, l, theta, p->tolerance, sweep + 1, stop, c->s);
@@ -728,12 +725,19 @@ extern "C" int gfc_ctx_fix(gfc_ctx *c, const gfc_params *p, const gfc_options *o
     }
     GFC_CHECK(cudaSetDevice(c->dev));
     long long l0 = c->launches;
-    if (opt->warm_start && opt->precision == GFC_PREC_MIXED) {
-        set_error("a warm start runs on the FP64 paths (not GFC_PREC_MIXED)");
-        r->status = GFC_ERR_ARG;
-        return GFC_ERR_ARG;
+    const bool mixed = opt->precision == GFC_PREC_MIXED && c->lat.cb;
+    if (opt->warm_start && mixed && !c->u0) {
+        set_error("context was created without GFC_CTX_MIXED");
+        r->status = GFC_ERR_STATE;
+        return GFC_ERR_STATE;
     }
     GFC_CHECK(cudaEventRecord(c->ev_a, c->s));
+    if (opt->warm_start && mixed) {
+        // the mixed path re-gauges the links as uploaded with the whole G at its
+        // switch to FP64: keep them before G0 is applied
+        GFC_CHECK(cudaMemcpyAsync(c->u0, c->u, (size_t)3 * c->lat.npar * c->lat.vh * 9 * sizeof(double2),
+                                  cudaMemcpyDeviceToDevice, c->s));
+    }
     if (opt->warm_start) {
         // the resident G is the starting transformation: fix G0 U G0^dagger (spatial
         // links now, temporal ones with the final G at the end) and keep accumulating
@@ -746,7 +750,7 @@ extern "C" int gfc_ctx_fix(gfc_ctx *c, const gfc_params *p, const gfc_options *o
     }
 
     int ret;
-    if (opt->precision == GFC_PREC_MIXED && c->lat.cb) {
+    if (mixed) {
         ret = fix_mixed(c, p, opt, r);
     } else if (opt->stop_rule == GFC_STOP_EVERY && (opt->precision == GFC_PREC_FP64_EXACT || !c->lat.cb)) {
         ret = fix_every_sweep_exact(c, p, opt, r);

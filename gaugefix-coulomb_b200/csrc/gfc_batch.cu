@@ -253,6 +253,76 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
     }
 }
 
+// The same persistent half-sweep with one warp per CTA (the shape of the fastest
+// single-lattice launches: 32-site blocks, 8-12 per SM).  A work item's BCHUNK sites
+// are swept as BCHUNK / 32 pieces of 32, one after the other, each with its six
+// links staged in shared memory (6 x NS x 32 x 16 B per CTA); a CTA never waits for
+// the slowest of several warps, and the item's e2 partials are summed over its
+// pieces per lane, then across the warp, in a fixed order.  Each thread stages into
+// and reads back from its own shared-memory slots only, so no CTA barrier is needed.
+template <class S, int MINB>
+__global__ void __launch_bounds__(32, MINB) k_bsweep_w(BState b) {
+    extern __shared__ __align__(16) unsigned char bstage[];
+    using T = typename S::T;
+    constexpr bool F64 = sizeof(T) == 8;
+    const int n = b.counts[F64 ? 1 : 0];
+    const int expect = F64 ? SS_FP64 : SS_FP32;
+    const int2 *items = F64 ? b.items64 : b.items32;
+    int *cursor = b.counts + (F64 ? 7 : 6);
+    const int lane = threadIdx.x;
+    // the previous half-sweep's reunitarisation flags have been consumed
+    if (!F64 && blockIdx.x == 0 && lane == 0) b.counts[8] = b.counts[9] = 0;
+    int it = 0;
+    if (lane == 0) it = atomicAdd(cursor, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    while (it < n) {
+        // the next item is requested while this one is swept
+        int ahead = 0;
+        if (lane == 0) ahead = atomicAdd(cursor, 1);
+        const int2 item = items[it];
+        const int gid = item.x, chunk = item.y;
+        const int st = *(volatile int *)&b.state[gid];
+        const bool verify = F64 && st == SS_VERIFY;
+        if (st == expect || verify) {
+            const int par = b.sweeps[gid] & 1;
+            const int track = verify ? 1 : (b.mflag[gid] & MF_NOW);
+            const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
+            const BSlot &sl = b.slots[slot];
+            const Lat &l = sl.l;
+            typename S::V *u, *g;
+            slot_fields<S>(sl, u, g);
+            const uint32_t vsh = l.vs >> 1;
+            double pre = 0.0, post = 0.0;
+#pragma unroll 1
+            for (int q = 0; q < BCHUNK / 32; q++) {
+                const uint32_t off = (uint32_t)chunk * BCHUNK + (uint32_t)q * 32 + lane;
+                if (off >= vsh) break;
+                double a = 0.0, z = 0.0;
+                if (verify)
+                    a = measure_site<S>(u, l, par, (uint32_t)t * vsh + off);
+                else
+                    fast_site_staged<S, 32, false>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, track,
+                                                   a, z, (typename S::V *)bstage);
+                pre += a;
+                post += z;
+            }
+            if (track) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    pre += __shfl_down_sync(0xffffffffu, pre, o);
+                    post += __shfl_down_sync(0xffffffffu, post, o);
+                }
+                if (lane == 0) {
+                    double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
+                    pp[0] = pre;
+                    pp[1] = post;
+                }
+            }
+        }
+        it = __shfl_sync(0xffffffffu, ahead, 0);
+    }
+}
+
 // After both sweep kernels of a half-sweep, one warp per swept timeslice: advances its
 // half-sweep count and e2 measurement schedule; where the half-sweep was measured,
 // sums the chunk partials in a fixed order (lane-strided, then a shuffle tree) and,
@@ -514,7 +584,7 @@ struct gfc_batch {
     int round_k = 8;
     BState captured{};
     int grid = 0, nsm = 0;
-    int minb32 = 4, minb64 = 3, stage64 = 1;
+    int minb32 = 11, minb64 = 11, stage64 = 1;   // one-warp CTAs, 11 per SM (measured fastest)
     // slot memory: a pool of its own that keeps freed memory mapped, so a slot
     // freed and another admitted costs no unmapping and remapping of device memory
     cudaMemPool_t pool = nullptr;
@@ -878,10 +948,26 @@ static void launch_bsweep_k(int grid, cudaStream_t st, const BState &bs) {
     kern<<<grid, BCHUNK, bytes, st>>>(bs);
 }
 
-// minb: minimum resident CTAs per SM (1..4); stage: FP64 links staged in shared
-// memory (two-row FP64 only; 72 KiB per CTA, so at most 3 CTAs per SM)
+template <class S, int MINB>
+static void launch_bsweep_w(int grid, cudaStream_t st, const BState &bs) {
+    constexpr size_t bytes = (size_t)6 * S::NS * 32 * 16;
+    auto kern = k_bsweep_w<S, MINB>;
+    static std::atomic<unsigned long long> done{0};
+    smem_attr_once(done, kern, bytes);
+    kern<<<grid, 32, bytes, st>>>(bs);
+}
+
+// minb: minimum resident CTAs per SM: 1..4 CTAs of BCHUNK threads (stage: FP64 links
+// staged in shared memory, two-row FP64 only; 72 KiB per CTA, so at most 3 CTAs per
+// SM), or 8, 11 or 12 one-warp CTAs with staged links (k_bsweep_w)
 template <class S>
 static void launch_bsweep(int minb, bool stage, int grid, cudaStream_t st, const BState &bs) {
+    switch (minb) {
+        case 8: return launch_bsweep_w<S, 8>(grid, st, bs);
+        case 11: return launch_bsweep_w<S, 11>(grid, st, bs);
+        case 12: return launch_bsweep_w<S, 12>(grid, st, bs);
+        default: break;
+    }
     if constexpr (sizeof(typename S::T) == 8) {
         if (stage) {
             switch (minb) {
@@ -909,7 +995,7 @@ static void enqueue_round(gfc_batch *b, const BState &bs) {
     for (int k = 0; k < b->round_k; k++) {
         // one resident wave of persistent CTAs: a CTA that had to wait for a slot
         // would start its share of the items late and stretch the tail
-        const int m64 = b->stage64 ? std::min(b->minb64, 3) : b->minb64;
+        const int m64 = b->stage64 && b->minb64 <= 4 ? std::min(b->minb64, 3) : b->minb64;
         launch_bsweep<S32>(b->minb32, false, b->nsm * b->minb32, st, bs);
         launch_bsweep<S64R>(m64, b->stage64 != 0, b->nsm * m64, st, bs);
         k_bslice<<<(b->nslices + 7) / 8, 256, 0, st>>>(bs);
@@ -1140,8 +1226,10 @@ extern "C" void *gfc_batch_stream(gfc_batch *b) { return b ? (void *)b->s : null
 
 // launch shape (minimum resident CTAs per SM) of the two sweep kernels and the
 // half-sweeps per captured round
+static bool valid_minb(int m) { return (m >= 1 && m <= 4) || m == 8 || m == 11 || m == 12; }
+
 extern "C" int gfc_batch_set_shape(gfc_batch *b, int minb32, int minb64, int round_sweeps) {
-    if (!b || minb32 < 1 || minb32 > 4 || minb64 < 1 || minb64 > 4 || round_sweeps < 1 || round_sweeps > 64)
+    if (!b || !valid_minb(minb32) || !valid_minb(minb64) || round_sweeps < 1 || round_sweeps > 64)
         return GFC_ERR_ARG;
     b->minb32 = minb32;
     b->minb64 = minb64;
@@ -1175,8 +1263,8 @@ extern "C" int gfc_batch_set_staging(gfc_batch *b, int stage64) {
 extern "C" int gfc_batch_get_shape(const gfc_batch *b, int *minb32, int *minb64, int *stage64, int *round_sweeps) {
     if (!b) return GFC_ERR_ARG;
     if (minb32) *minb32 = b->minb32;
-    if (minb64) *minb64 = b->stage64 ? std::min(b->minb64, 3) : b->minb64;
-    if (stage64) *stage64 = b->stage64;
+    if (minb64) *minb64 = b->stage64 && b->minb64 <= 4 ? std::min(b->minb64, 3) : b->minb64;
+    if (stage64) *stage64 = b->minb64 > 4 ? 1 : b->stage64;
     if (round_sweeps) *round_sweeps = b->round_k;
     return GFC_OK;
 }
@@ -1187,7 +1275,8 @@ extern "C" int gfc_batch_get_shape(const gfc_batch *b, int *minb32, int *minb64,
 // captured round.  The batch must have no activated slot; the scratch slot is
 // removed again.  times (may be NULL, GFC_BATCH_TUNE_SLOTS entries) receives seconds
 // per half-sweep: [0..2] FP32 minb 2,3,4; [3..7] FP64 (minb, staged) (2,0) (3,0)
-// (4,0) (2,1) (3,1); [8..10] rounds of 4, 8, 16 half-sweeps.
+// (4,0) (2,1) (3,1); [8..10] rounds of 4, 8, 16 half-sweeps; [11..13] FP32 and
+// [14..16] FP64 one-warp CTAs, 8, 11, 12 per SM.
 extern "C" int gfc_batch_autotune(gfc_batch *b, int ns, int nt, double *times) {
     if (!b) return GFC_ERR_ARG;
     for (int k = 0; k < b->max_slots; k++)
@@ -1230,22 +1319,23 @@ extern "C" int gfc_batch_autotune(gfc_batch *b, int ns, int nt, double *times) {
         // FP32 sweep
         if ((rc = gfc_batch_activate(b, slot, GFC_PREC_MIXED))) break;
         double best = 1e30;
-        const int m32[3] = {2, 3, 4};
-        for (int q = 0; q < 3 && !rc; q++) {
+        const int m32[6] = {2, 3, 4, 8, 11, 12}, i32[6] = {0, 1, 2, 11, 12, 13};
+        for (int q = 0; q < 6 && !rc; q++) {
             gfc_batch_set_shape(b, m32[q], save64, 4);
-            rc = time_rounds(GFC_PREC_MIXED, t[q]);
-            if (!rc && t[q] < best) best = t[q], best32 = m32[q];
+            rc = time_rounds(GFC_PREC_MIXED, t[i32[q]]);
+            if (!rc && t[i32[q]] < best) best = t[i32[q]], best32 = m32[q];
         }
         if (rc) break;
         // FP64 sweep
         if ((rc = gfc_batch_activate(b, slot, GFC_PREC_FP64_FAST))) break;
         best = 1e30;
-        const int m64[5] = {2, 3, 4, 2, 3}, st64[5] = {0, 0, 0, 1, 1};
-        for (int q = 0; q < 5 && !rc; q++) {
+        const int m64[8] = {2, 3, 4, 2, 3, 8, 11, 12}, st64[8] = {0, 0, 0, 1, 1, 1, 1, 1};
+        const int i64[8] = {3, 4, 5, 6, 7, 14, 15, 16};
+        for (int q = 0; q < 8 && !rc; q++) {
             gfc_batch_set_shape(b, best32, m64[q], 4);
             gfc_batch_set_staging(b, st64[q]);
-            rc = time_rounds(GFC_PREC_FP64_FAST, t[3 + q]);
-            if (!rc && t[3 + q] < best) best = t[3 + q], best64 = m64[q], bests = st64[q];
+            rc = time_rounds(GFC_PREC_FP64_FAST, t[i64[q]]);
+            if (!rc && t[i64[q]] < best) best = t[i64[q]], best64 = m64[q], bests = st64[q];
         }
         if (rc) break;
         // half-sweeps per round (FP64 work; the per-round compaction is amortised)

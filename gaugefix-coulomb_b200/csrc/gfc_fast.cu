@@ -266,6 +266,22 @@ __global__ void k_to_f64(const float4 *__restrict__ src, double2 *__restrict__ d
     for (int e = 0; e < 9; e++) q[(size_t)e * stride] = m.e[e];
 }
 
+// G <- G1 . G on FP64 full SoA blocks ([9][stride] per block), projected back onto
+// SU(3): a warm start's G0 composed with the transformation of the FP32 phase
+__global__ void k_left_mul_gt(const double2 *__restrict__ g1, double2 *__restrict__ g, uint32_t stride,
+                              uint32_t nblk) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+    if (i >= stride || k >= nblk) return;
+    const size_t o = (size_t)k * 9 * stride + i;
+    Mt<double> a, b, c;
+    S64::load(g1 + o, stride, a);
+    S64::load(g + o, stride, b);
+    fprod_left<S64, double>(a, b, c);
+    if (!fproject(c)) fidentity(c);
+#pragma unroll
+    for (int e = 0; e < 9; e++) g[o + (size_t)e * stride] = c.e[e];
+}
+
 // FP64 full SoA ([9][stride] per block) -> FP64 two-row SoA ([6][stride])
 __global__ void k_pack2(const double2 *__restrict__ src, double2 *__restrict__ dst, uint32_t stride, uint32_t nblk) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
@@ -746,20 +762,39 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     const double tol_e2 = p->gfix_proxy == GFC_PROXY_THETA ? 6.0 * p->tolerance : p->tolerance;
     const double sw = std::max(o->switch_e2 > 0 ? o->switch_e2 : 1e-9, tol_e2);
     const size_t mat = (size_t)l.npar * l.vh * 9;
-    // keep the FP64 links of the start; they are re-gauged at the switch
-    GFC_CHECK(cudaMemcpyAsync(c->u0, c->u, 3 * mat * sizeof(double2), cudaMemcpyDeviceToDevice, c->s));
+    // keep the FP64 links of the start; they are re-gauged at the switch (a warm
+    // start kept the links as uploaded, before G0 was applied, in u0 already)
+    if (!o->warm_start)
+        GFC_CHECK(cudaMemcpyAsync(c->u0, c->u, 3 * mat * sizeof(double2), cudaMemcpyDeviceToDevice, c->s));
     {
         dim3 gu((l.vh + 255) / 256, 3 * l.npar), gg((l.vh + 255) / 256, l.npar);
         k_to_f32<<<gu, 256, 0, c->s>>>(c->u, (float4 *)c->u32, l.vh, 3 * l.npar);
         k_identity32<<<gg, 256, 0, c->s>>>((float4 *)c->g32, l.vh, l.npar);
         c->launches += 2;
     }
-    // FP32 bulk
+    // FP32 bulk, in pieces of fp32_refresh half-sweeps when refreshing
     const unsigned reunit32 = std::min<unsigned>(p->sweeps_to_reunitarization, 50u);
+    const int maxs = (int)p->max_sweeps_to_fix, K = o->fp32_refresh > 0 ? o->fp32_refresh : 0;
     int done = 0, below = -1;
-    rc = run_until<S32>(c, (float4 *)c->u32, (float4 *)c->g32, 0, (int)p->max_sweeps_to_fix, sw,
-                        (double)p->omega_OR, p->hits, reunit32, o->dense_check, &done, &below);
-    if (rc) return rc;
+    for (;;) {
+        const int lim = K ? std::min(maxs, done + K) : maxs;
+        int d = done;
+        rc = run_until<S32>(c, (float4 *)c->u32, (float4 *)c->g32, done, lim, sw, (double)p->omega_OR, p->hits,
+                            reunit32, o->dense_check, &d, &below);
+        if (rc) return rc;
+        done = d;
+        if (below >= 0 || !K || done >= maxs) break;
+        // refresh: G = G32 G in FP64 (projected), links G U0 G^dagger in FP64, rounded
+        // to FP32 again; the FP32 G restarts from the identity
+        if ((rc = ensure_2row(c))) return rc;
+        dim3 gg((l.vh + 255) / 256, l.npar), gu((l.vh + 255) / 256, 3 * l.npar);
+        k_to_f64<<<gg, 256, 0, c->s>>>((const float4 *)c->g32, c->u64r, l.vh, l.npar);
+        k_left_mul_gt<<<gg, 256, 0, c->s>>>(c->u64r, c->g, l.vh, l.npar);
+        launch_apply_gt_spatial(c->u, c->u0, c->g, l, c->s);
+        k_to_f32<<<gu, 256, 0, c->s>>>(c->u, (float4 *)c->u32, l.vh, 3 * l.npar);
+        k_identity32<<<gg, 256, 0, c->s>>>((float4 *)c->g32, l.vh, l.npar);
+        c->launches += 5;
+    }
     r->sweeps_fp32 = done;
     if (below < 0) {
         r->sweeps = done;
@@ -767,17 +802,26 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
         return GFC_FIX_NOT_CONVERGED;
     }
     // switch: G in FP64 (rebuilt and projected), U = G U0 G^dagger from the FP64 start
+    if ((rc = ensure_2row(c))) return rc;
     {
         dim3 gg((l.vh + 255) / 256, l.npar);
-        k_to_f64<<<gg, 256, 0, c->s>>>((const float4 *)c->g32, c->g, l.vh, l.npar);
-        c->launches++;
+        if (o->warm_start || K) {
+            // G = G1 G0: G1 of the FP32 phase (FP64, in the two-row buffer, which
+            // is free until the refinement) times the starting G0 (a warm start's,
+            // or the one accumulated by the refreshes)
+            k_to_f64<<<gg, 256, 0, c->s>>>((const float4 *)c->g32, c->u64r, l.vh, l.npar);
+            k_left_mul_gt<<<gg, 256, 0, c->s>>>(c->u64r, c->g, l.vh, l.npar);
+            c->launches += 2;
+        } else {
+            k_to_f64<<<gg, 256, 0, c->s>>>((const float4 *)c->g32, c->g, l.vh, l.npar);
+            c->launches++;
+        }
     }
     launch_apply_gt_spatial(c->u, c->u0, c->g, l, c->s);
     c->launches++;
     // FP64 refinement
     unsigned reunit64 = o->refine_reunit ? o->refine_reunit : p->sweeps_to_reunitarization;
     int done64 = 0;
-    if ((rc = ensure_2row(c))) return rc;
     pack_2row(c);
     rc = run_until<S64R>(c, c->u64r, c->g64r, done, (int)p->max_sweeps_to_fix, tol_e2, (double)p->omega_OR,
                          p->hits, reunit64, o->dense_check, &done64, &below);

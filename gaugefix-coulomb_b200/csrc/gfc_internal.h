@@ -33,7 +33,7 @@ inline void smem_attr_once(std::atomic<unsigned long long> &done, K kern, size_t
 
 // ---- exact FP64 kernels (gfc_kernels_exact.cu)
 // stop (optional): a device stop word; once set, the launch does nothing
-void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
+int launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
                         cudaStream_t s, int shape = 0, const unsigned *stop = nullptr);
 int exact_num_shapes();
 void launch_reunitarize(double2 *base, uint32_t stride, uint32_t nblk, unsigned *status, cudaStream_t s);

@@ -169,24 +169,34 @@ static void launch_exact_staged(const Lat &l, double2 *u, double2 *g, int par, d
     kern<<<(l.vh + BLOCK - 1) / BLOCK, BLOCK, bytes, s>>>(u, g, l, par, omega, hits, stop);
 }
 
-// Odd ns: same-parity sites meet across the periodic boundary, so updates inside
-// a timeslice depend on their order.  One thread per timeslice visits the slice in
-// the reference's z, y, x order; distinct timeslices share no spatial link.
-__global__ void k_sweep_exact_serial(double2 *__restrict__ u, double2 *__restrict__ g, Lat l, int sweep,
-                                     double omega, unsigned hits, const unsigned *stop) {
+// Odd ns: same-parity sites meet across the periodic boundary, so the updates of a
+// half-sweep depend on their order; the reference visits a timeslice in z, y, x
+// order (LOOP_SPATIAL).  Two sites of one parity share a link only across the
+// boundary: a site with coordinate 0 in direction d and the one with ns - 1 there
+// (other coordinates equal), and the reference always updates the first before the
+// second.  Ordering the sites by their number of coordinates equal to ns - 1 (the
+// boundary level, 0..3) therefore puts every such pair in consecutive levels, in
+// the reference's order, and no two sites of one level share a link: sweeping
+// level 0, then 1, 2 and 3, each level in parallel, gives every site the links the
+// sequential sweep gives it, bit for bit.  Lexicographic layout, one thread per site.
+__global__ void __launch_bounds__(128) k_sweep_exact_level(double2 *__restrict__ u, double2 *__restrict__ g, Lat l,
+                                                           int sweep, int level, double omega, unsigned hits,
+                                                           const unsigned *stop) {
     if (stop && *(volatile const unsigned *)stop) return;
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (uint32_t)l.nt) return;
-    for (uint32_t r = 0; r < l.vs; r++) {
-        Coord c = coord_lex(l, t * l.vs + r);
-        int even = !((c.x ^ c.y ^ c.z ^ c.t) & 1u);
-        if (even ^ (sweep & 1)) site_update_exact<false>(u, g, l, 0, c, omega, hits);
-    }
+    const uint32_t L = blockIdx.x * 128 + threadIdx.x;
+    if (L >= l.v) return;
+    Coord c = coord_lex(l, L);
+    const int even = !((c.x ^ c.y ^ c.z ^ c.t) & 1u);
+    if (!(even ^ (sweep & 1))) return;   // BLACKRED_SWEEP (gauge_fixing.c:42)
+    const uint32_t e = (uint32_t)l.ns - 1;
+    if ((int)(c.x == e) + (int)(c.y == e) + (int)(c.z == e) != level) return;
+    site_update_exact<false>(u, g, l, 0, c, omega, hits);
 }
 
 int exact_num_shapes() { return 5; }
 
-void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
+// returns the number of kernels launched
+int launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double omega, unsigned hits,
                         cudaStream_t s, int shape, const unsigned *stop) {
     if (l.cb) {
         int par = sweep & 1;  // BLACKRED_SWEEP: even sites on even sweeps (gauge_fixing.c:42)
@@ -208,9 +218,12 @@ void launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double 
                 break;
         }
     } else {
-        unsigned blocks = (l.nt + 31) / 32;
-        k_sweep_exact_serial<<<blocks, 32, 0, s>>>(u, g, l, sweep, omega, hits, stop);
+        const unsigned blocks = (l.v + 127) / 128;
+        for (int level = 0; level < 4; level++)
+            k_sweep_exact_level<<<blocks, 128, 0, s>>>(u, g, l, sweep, level, omega, hits, stop);
+        return 4;
     }
+    return 1;
 }
 
 // ----------------------------------------------------------- reunitarise --
@@ -463,8 +476,8 @@ void launch_functional(const double2 *u, const Lat &l, double *part, double *out
 }  // namespace gfc
 
 // Architecture of the device code the runtime loaded for this library on `device`
-// (cudaFuncGetAttributes of the exact half-sweep kernel): binaryVersion 100 is
-// sm_100a machine code; ptxVersion 0 means no PTX was embedded for JIT.
+// (cudaFuncGetAttributes of one of its kernels): binaryVersion 100 is sm_100 machine
+// code, ptxVersion the virtual architecture it was compiled from.
 extern "C" int gfc_device_code_version(int device, int *binary_version, int *ptx_version) {
     if (!binary_version || !ptx_version) {
         gfc::set_error("gfc_device_code_version: null output");

@@ -53,6 +53,7 @@ class Options(ctypes.Structure):
         ("block_threads", ctypes.c_int),
         ("dense_check", ctypes.c_int),
         ("warm_start", ctypes.c_int),
+        ("fp32_refresh", ctypes.c_int),
     ]
 
 
@@ -399,6 +400,12 @@ def gaugefix_overrelaxation(U, G, ns, nt, params=None, opts=None, device=0):
 
 
 # ---------------------------------------------------------------- batches --
+def _batch_tune_times(t):
+    return {"fp32_minb_2_3_4": list(t[0:3]), "fp64_minb_staged_20_30_40_21_31": list(t[3:8]),
+            "round_4_8_16": list(t[8:11]), "fp32_warp_ctas_8_11_12": list(t[11:14]),
+            "fp64_warp_ctas_8_11_12": list(t[14:17])}
+
+
 def _bind_batch():
     P, I, D, S = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
     IP = ctypes.POINTER(ctypes.c_int)
@@ -548,10 +555,9 @@ class Batch:
 
     def autotune(self, ns, nt):
         """Time the launch shapes on a scratch ns^3 x nt lattice; keep the fastest."""
-        t = (ctypes.c_double * 11)()
+        t = (ctypes.c_double * 17)()
         _check(lib.gfc_batch_autotune(self.h, ns, nt, t), "gfc_batch_autotune")
-        return {"fp32_minb_2_3_4": list(t[0:3]), "fp64_minb_staged_20_30_40_21_31": list(t[3:8]),
-                "round_4_8_16": list(t[8:11])}
+        return _batch_tune_times(t)
 
     @property
     def kernel_launches(self):
@@ -695,9 +701,9 @@ class Server:
     def autotune(self, ns, nt):
         """Launch shapes of the server's batch, timed on a scratch ns^3 x nt lattice
         (before requests are admitted)."""
-        t = (ctypes.c_double * 11)()
+        t = (ctypes.c_double * 17)()
         _check(lib.gfc_batch_autotune(lib.gfc_server_batch(self.h), ns, nt, t), "gfc_batch_autotune")
-        return list(t)
+        return _batch_tune_times(t)
 
     def batch_stream(self):
         return lib.gfc_batch_stream(lib.gfc_server_batch(self.h))

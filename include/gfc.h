@@ -97,7 +97,13 @@ typedef struct {
                                  transformation: the fix works on G U G^dagger and the G
                                  it returns includes it (loadGaugeTransf +
                                  applyGaugeTransformationU, fields_io.c:309-402,
-                                 fields.c:375-435, then the fix); FP64 paths only      */
+                                 fields.c:375-435, then the fix); every precision (the
+                                 mixed path re-gauges the uploaded links with G1 G0
+                                 at its switch to FP64)                              */
+    int    fp32_refresh;      /* mixed: every n FP32 half-sweeps fold the FP32 G into an
+                                 FP64 G and rebuild the FP32 links from it as G U0
+                                 G^dagger in FP64, so FP32 rounding does not accumulate
+                                 in the links (0: off)                                */
 } gfc_options;
 
 void gfc_options_default(gfc_options *o);
@@ -146,8 +152,9 @@ typedef struct gfc_ctx gfc_ctx;
 
 const char *gfc_last_error(void);
 /* Architecture of the library's device code as loaded on `device`
- * (cudaFuncGetAttributes): binary_version 100 = sm_100a machine code, ptx_version 0
- * = no PTX embedded.  No counterpart in the reference (it has no device code). */
+ * (cudaFuncGetAttributes): binary_version 100 = sm_100 machine code, ptx_version =
+ * the virtual architecture it was compiled for (100).  No counterpart in the
+ * reference (it has no device code). */
 int  gfc_device_code_version(int device, int *binary_version, int *ptx_version);
 /* page-locked host memory for fast transfers (cudaMallocHost / cudaFreeHost) */
 void *gfc_host_alloc(size_t bytes);
@@ -289,7 +296,9 @@ int    gfc_batch_status(gfc_batch *b, unsigned *status);
 int    gfc_batch_slice_sweeps(gfc_batch *b, int slot, int *out);
 long long gfc_batch_kernel_launches(const gfc_batch *b);
 void  *gfc_batch_stream(gfc_batch *b);
-/* minimum resident CTAs per SM of the FP32 / FP64 sweep kernels (1..4) and half-sweeps per round */
+/* minimum resident CTAs per SM of the FP32 / FP64 sweep kernels and half-sweeps per
+ * round: 1..4 CTAs of 128 threads, or 8, 11 or 12 one-warp CTAs (links staged in
+ * shared memory, the 128 sites of a work item swept 32 at a time) */
 int    gfc_batch_set_shape(gfc_batch *b, int minb32, int minb64, int round_sweeps);
 /* FP64 batch sweep with the links staged in shared memory (1, default) or not (0) */
 int    gfc_batch_set_staging(gfc_batch *b, int stage64);
@@ -298,8 +307,9 @@ int    gfc_batch_get_shape(const gfc_batch *b, int *minb32, int *minb64, int *st
  * (FP32 resident CTAs per SM, FP64 resident CTAs and staging, half-sweeps per round).
  * Needs a batch without activated slots.  times (may be NULL): seconds per half-sweep,
  * [0..2] FP32 minb 2,3,4; [3..7] FP64 (minb, staged) (2,0) (3,0) (4,0) (2,1) (3,1);
- * [8..10] rounds of 4, 8, 16 half-sweeps. */
-#define GFC_BATCH_TUNE_SLOTS 11
+ * [8..10] rounds of 4, 8, 16 half-sweeps; [11..13] FP32 one-warp CTAs 8, 11, 12 per
+ * SM; [14..16] FP64 one-warp CTAs 8, 11, 12 per SM. */
+#define GFC_BATCH_TUNE_SLOTS 17
 int    gfc_batch_autotune(gfc_batch *b, int ns, int nt, double *times);
 /* rounds until every activated slot retired (or max_sweeps), then finalise them;
  * reports indexed by slot; returns the number of rounds */

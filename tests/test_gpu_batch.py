@@ -40,11 +40,21 @@ def test_device_generator_matches_host():
     np.testing.assert_allclose(Ud, Uh, atol=1e-13)
 
 
+# launch shapes (minimum resident CTAs per SM of the FP32 and FP64 sweeps): the
+# default 128-thread CTAs, and one-warp CTAs that sweep a 128-site work item 32
+# sites at a time (the lattices below have 16, 108 and 256 sites per timeslice and
+# parity: ragged pieces and items)
+SHAPES = [None, (12, 12), (8, 11)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
 @pytest.mark.parametrize("precision", [gfc.PREC_MIXED, gfc.PREC_FP64_FAST])
-def test_uneven_batch_fixes_every_lattice(precision):
+def test_uneven_batch_fixes_every_lattice(precision, shape):
     geoms = [(4, 8, 71, 0.4), (6, 6, 72, 0.7), (8, 12, 73, 0.5)]
     U0 = {}
     with gfc.Batch(max_sites=10 ** 6, max_slots=8, max_nt=16) as b:
+        if shape:
+            b.set_shape(shape[0], shape[1], 8)
         slots = []
         for ns, nt, seed, scale in geoms:
             s = b.add(ns, nt)
@@ -80,7 +90,8 @@ def test_uneven_batch_fixes_every_lattice(precision):
         assert b.status() == 0
 
 
-def test_same_result_alone_and_in_the_mix():
+@pytest.mark.parametrize("shape", SHAPES)
+def test_same_result_alone_and_in_the_mix(shape):
     """Continuous batching: a lattice admitted while others are running gets exactly
     the result it gets alone."""
     ns, nt = 6, 8
@@ -88,6 +99,8 @@ def test_same_result_alone_and_in_the_mix():
     other = gfc.synth_config(8, 8, 92, 0.6)
     p, o = params(), gfc.options(precision=gfc.PREC_MIXED)
     with gfc.Batch(max_sites=10 ** 6, max_slots=4, max_nt=16) as b:
+        if shape:
+            b.set_shape(shape[0], shape[1], 8)
         s = b.add(ns, nt)
         b.upload(s, U, 8, False)
         b.activate(s, gfc.PREC_MIXED)
@@ -95,6 +108,8 @@ def test_same_result_alone_and_in_the_mix():
         G_alone = b.download_gt(s)
         sw_alone = b.slice_sweeps(s)
     with gfc.Batch(max_sites=10 ** 6, max_slots=4, max_nt=16) as b:
+        if shape:
+            b.set_shape(shape[0], shape[1], 8)
         s_other = b.add(8, 8)
         b.upload(s_other, other, 8, False)
         b.activate(s_other, gfc.PREC_MIXED)
@@ -132,7 +147,8 @@ def test_batch_autotune_then_fix():
         times = b.autotune(8, 12)
         assert all(t > 0 for v in times.values() for t in v)
         shape = b.shape()
-        assert 2 <= shape["minb32"] <= 4 and shape["round_sweeps"] in (4, 8, 16)
+        assert shape["minb32"] in (2, 3, 4, 8, 11, 12) and shape["round_sweeps"] in (4, 8, 16)
+        assert shape["minb64"] in (2, 3, 4, 8, 11, 12)
         with pytest.raises(gfc.GFCError):
             s = b.add(6, 8)
             b.upload(s, gfc.synth_config(6, 8, 5, 0.5), 8, False)

@@ -1,0 +1,201 @@
+"""Parity at the sizes of the workloads, against the reference's own complete fixes.
+
+Fixtures (tests/golden/full_cases.json, made by tests/golden/make_golden.py --full
+from the reference built from its sources): 32^3x64 stored FP64 (seed 2, H scale
+0.5) and 48^3x96 stored FP32 and converted on load (seed 3, H scale 0.7), both
+fixed to e2 <= 1e-15 with the reference's defaults (omega 1.95, 2 hits,
+reunitarisation every 250 half-sweeps, check schedule with estimate 1000).
+
+* The reference-arithmetic path returns the reference's G and spatial links bit
+  for bit, after the same number of half-sweeps (G after half-sweep 700 too), and
+  matches the gauge functional F at every traced half-sweep to 1e-12 relative and
+  e2 to 1e-11: the reference sums e2 in an OpenMP reduction over timeslices with
+  a dynamic schedule, whose order (and so its last digits) changes from run to
+  run; from the same links the two sums differ by up to 4.6e-12 relative.
+* The fast FP64 path (FMA, direct SU(2) accumulation, two stored rows) and the
+  mixed FP32 -> FP64 path round differently, so they are held to what the
+  reference's result pins:
+  - F at every traced half-sweep to 1e-12 relative;
+  - e2 at every traced half-sweep to 1e-12 relative plus the Cauchy-Schwarz bound
+    2 sqrt(e2) d + d^2 for algebra components that differ by d = 1e-12 (rms): once
+    e2 is small, links that agree to rounding cannot give e2 to 1e-12 relative;
+  - G after 700 half-sweeps and at the end of a fix on the reference's check
+    schedule element-wise to 1e-10 (same sweep count);
+  - from an every-half-sweep stop: e2 <= 1e-15, F to 1e-12 and plaquettes to 1e-13
+    of the reference's, the plaquettes unchanged by the fix to 1e-13, and G equal to
+    the reference's to 1e-6 once a rotation constant on each timeslice (the residual
+    gauge freedom, along which the rounding of the FP32 phase drifts) is removed.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import gfc
+import oracle_ref as orc
+from conftest import GOLDEN
+from gauge_util import global_rotation_residual
+
+pytestmark = pytest.mark.gpu
+
+with open(os.path.join(GOLDEN, "full_cases.json")) as _f:
+    FULL = {c["name"]: c for c in json.load(_f)}
+
+D_RMS = 1e-12   # rms difference of the algebra components of div A allowed
+
+
+class _Files(dict):
+    """The workload files' bytes (big endian, as stored) in page-locked memory,
+    made on first use."""
+
+    def __missing__(self, name):
+        c = FULL[name]
+        U = gfc.synth_config(c["ns"], c["nt"], c["seed"], c["scale"])
+        b = gfc.PinnedBuffer(U.size * c["in_bytes"])
+        b.view(">f8" if c["in_bytes"] == 8 else ">f4")[:] = U
+        self[name] = b
+        return b
+
+
+@pytest.fixture(scope="module")
+def raw():
+    files = _Files()
+    yield files
+    for b in files.values():
+        b.close()
+
+
+def load(lat, c, raw):
+    lat.upload_links(raw[c["name"]].array, c["in_bytes"], byteswap=True)
+    lat.reunitarize()
+
+
+def sample(G, c):
+    V = c["ns"] ** 3 * c["nt"]
+    return G.reshape(V, 18)[np.arange(0, V, c["sample_stride"])]
+
+
+@pytest.mark.parametrize("name", list(FULL))
+def test_exact_path_full_size_bit_for_bit(raw, name):
+    c = FULL[name]
+    with gfc.Lattice(c["ns"], c["nt"]) as lat:
+        load(lat, c, raw)
+        ps0, pt0 = lat.plaquette()
+        rc, rep = lat.fix(gfc.default_params(tolerance=1e-15), gfc.options(precision=gfc.PREC_FP64_EXACT))
+        ps1, pt1 = lat.plaquette()
+        G = lat.download_gt()
+        U = lat.download_links()
+    assert rc == c["sweeps"]
+    assert orc.sha(G) == c["gt_sha256"], np.abs(sample(G, c) - np.load(
+        os.path.join(GOLDEN, f"{name}_gt_sample.npy"))[1]).max()
+    assert orc.sha(U.reshape(-1, 4, 18)[:, 1:4, :]) == c["u_spatial_sha256"]
+    assert rep.final_residue == pytest.approx(c["final_residue"], rel=1e-12)
+    assert rep.functional == pytest.approx(c["F"], rel=1e-12)
+    assert ps0 == pytest.approx(c["plaq_spatial_0"], abs=1e-13) and pt0 == pytest.approx(c["plaq_temporal_0"],
+                                                                                          abs=1e-13)
+    assert ps1 == pytest.approx(c["plaq_spatial"], abs=1e-13) and pt1 == pytest.approx(c["plaq_temporal"], abs=1e-13)
+
+
+def run_trace(lat, c, precision):
+    """Half-sweeps 1..last traced one on the reference's reunitarisation period;
+    returns e2 and F at the traced half-sweeps and the G sample after dump_sweep."""
+    trace = np.load(os.path.join(GOLDEN, f"{c['name']}_trace.npy"))
+    points = sorted(set(int(s) for s in trace[1:, 0]) | {c["dump_sweep"]})
+    e2, F, gdump = {}, {}, None
+    k = 0
+    for target in points:
+        while k < target:
+            n = min(target - k, 250 - k % 250)
+            lat.halfsweeps(k, n, 1.95, 2, precision)
+            k += n
+            if k % 250 == 0 and k < target:
+                lat.reunitarize()
+                lat.reunitarize_gt()
+        # the reference records e2 and F before the reunitarisation due at this
+        # half-sweep, and dumps G after it
+        e2[k], _ = lat.e2_theta()
+        F[k] = lat.functional()
+        if k % 250 == 0:
+            lat.reunitarize()
+            lat.reunitarize_gt()
+        if k == c["dump_sweep"]:
+            gdump = sample(lat.download_gt(), c)
+    return trace, e2, F, gdump
+
+
+@pytest.mark.parametrize("precision", [gfc.PREC_FP64_EXACT, gfc.PREC_FP64_FAST])
+def test_per_half_sweep_trace_32x64(raw, precision):
+    """e2 and F after the first 20 half-sweeps and every 50th to 1050 (32^3x64),
+    and G after half-sweep 700, against the reference's run."""
+    c = FULL["cfg1_32x64"]
+    gold = np.load(os.path.join(GOLDEN, "cfg1_32x64_gt_sample.npy"))
+    with gfc.Lattice(c["ns"], c["nt"]) as lat:
+        load(lat, c, raw)
+        lat.set_identity_gt()
+        trace, e2, F, gdump = run_trace(lat, c, precision)
+    rows = [(int(s), e, f) for s, e, f in trace[1:]]
+    de2 = np.array([abs(e2[s] - e) for s, e, _ in rows])
+    ref_e2 = np.array([e for _, e, _ in rows])
+    dF = np.array([abs(F[s] - f) / abs(f) for s, _, f in rows])
+    dG = np.abs(gdump - gold[0]).max()
+    print(f"\nprecision {precision}: max rel dF {dF.max():.2e}; max rel de2 {(de2 / ref_e2).max():.2e}; "
+          f"max |dG| after 700: {dG:.2e}")
+    for (s, e, _), d, f in zip(rows, de2, dF):
+        print(f"  half-sweep {s:5d}  e2_ref {e:.3e}  |de2| {d:.2e}  rel {d / e:.1e}  "
+              f"d_rms >= {d / (2 * np.sqrt(e)):.1e}  rel dF {f:.1e}")
+    assert (dF <= 1e-12).all()
+    if precision == gfc.PREC_FP64_EXACT:
+        assert (de2 <= 1e-11 * ref_e2).all()
+        assert dG == 0.0
+    else:
+        assert (de2 <= 1e-12 * ref_e2 + 2 * np.sqrt(ref_e2) * D_RMS + D_RMS ** 2).all()
+        assert dG <= 1e-10
+
+
+@pytest.mark.parametrize("precision", [gfc.PREC_FP64_FAST])
+def test_fast_paths_reference_schedule_full_size(raw, precision):
+    """On the reference's check schedule the fast FP64 path stops after the same
+    number of half-sweeps and returns the reference's G to 1e-10 element-wise."""
+    c = FULL["cfg1_32x64"]
+    gold = np.load(os.path.join(GOLDEN, "cfg1_32x64_gt_sample.npy"))
+    with gfc.Lattice(c["ns"], c["nt"]) as lat:
+        load(lat, c, raw)
+        rc, rep = lat.fix(gfc.default_params(tolerance=1e-15),
+                          gfc.options(precision=precision, stop_rule=gfc.STOP_REFERENCE))
+        G = lat.download_gt()
+    dG = np.abs(sample(G, c) - gold[1]).max()
+    print(f"\nprecision {precision}: {rc} half-sweeps (reference {c['sweeps']}), max |dG| {dG:.2e}, "
+          f"e2 {rep.final_residue:.3e} (reference {c['final_residue']:.3e})")
+    assert rc == c["sweeps"]
+    assert dG <= 1e-10
+    assert rep.final_residue <= 1e-15
+    assert rep.functional == pytest.approx(c["F"], rel=1e-12)
+
+
+@pytest.mark.parametrize("name", list(FULL))
+@pytest.mark.parametrize("precision", [gfc.PREC_FP64_FAST, gfc.PREC_FP64_FULL, gfc.PREC_MIXED])
+def test_every_sweep_stop_full_size(raw, name, precision):
+    """Stopping at the first half-sweep with e2 <= 1e-15: the final e2, the gauge
+    functional and the plaquettes against the reference's fix of the same input."""
+    c = FULL[name]
+    with gfc.Lattice(c["ns"], c["nt"], mixed=precision == gfc.PREC_MIXED) as lat:
+        load(lat, c, raw)
+        ps0, pt0 = lat.plaquette()
+        rc, rep = lat.fix(gfc.default_params(tolerance=1e-15),
+                          gfc.options(precision=precision, stop_rule=gfc.STOP_EVERY,
+                                      refine_reunit=10 if precision == gfc.PREC_MIXED else 0))
+        ps1, pt1 = lat.plaquette()
+        e2, _ = lat.e2_theta()
+        G = sample(lat.download_gt(), c)
+    gold = np.load(os.path.join(GOLDEN, f"{name}_gt_sample.npy"))[1]
+    sites = np.arange(0, c["ns"] ** 3 * c["nt"], c["sample_stride"])
+    res, drift = global_rotation_residual(G, gold, sites // c["ns"] ** 3)
+    print(f"\n{name} precision {precision}: {rc} half-sweeps, e2 {e2:.3e}, "
+          f"F - F_ref {rep.functional - c['F']:.2e}, plaquette drift {max(abs(ps1 - ps0), abs(pt1 - pt0)):.1e}, "
+          f"max |dG| {np.abs(G - gold).max():.1e}, after removing h(t) {res:.1e} (|h(t) - 1| <= {drift:.1e})")
+    assert rc > 0 and rep.final_residue <= 1e-15 and e2 <= 1e-15
+    assert rep.functional == pytest.approx(c["F"], rel=1e-12)
+    assert abs(ps1 - ps0) <= 1e-13 and abs(pt1 - pt0) <= 1e-13
+    assert ps1 == pytest.approx(c["plaq_spatial"], abs=1e-13) and pt1 == pytest.approx(c["plaq_temporal"], abs=1e-13)
+    assert res <= 1e-6

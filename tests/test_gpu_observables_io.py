@@ -5,6 +5,7 @@ import pytest
 
 import gfc
 import oracle_ref as orc
+from gauge_util import global_rotation_residual
 
 pytestmark = pytest.mark.gpu
 
@@ -119,7 +120,8 @@ def test_apply_gt_matches_oracle_bitwise():
 
 
 @pytest.mark.parametrize("precision,stop", [(gfc.PREC_FP64_EXACT, gfc.STOP_REFERENCE),
-                                            (gfc.PREC_FP64_FAST, gfc.STOP_EVERY)])
+                                            (gfc.PREC_FP64_FAST, gfc.STOP_EVERY),
+                                            (gfc.PREC_MIXED, gfc.STOP_EVERY)])
 def test_warm_start(precision, stop):
     """Fixing from a saved transformation G0: the links fixed are G0 U G0^dagger and
     the G returned is the whole transformation (the oracle: applyGaugeTransformationU,
@@ -132,7 +134,7 @@ def test_warm_start(precision, stop):
     orc.apply_gt(U1, G0, ns, nt)
     Gf = np.zeros_like(G0)
     rc_o = orc.fix(U1, Gf, ns, nt, tol=1e-15)[0]
-    with gfc.Lattice(ns, nt) as lat:
+    with gfc.Lattice(ns, nt, mixed=precision == gfc.PREC_MIXED) as lat:
         lat.upload_links(U0, 8, False)
         lat.upload_gt(G0, 8, False)
         rc, rep = lat.fix(gfc.default_params(tolerance=1e-15),
@@ -140,10 +142,19 @@ def test_warm_start(precision, stop):
         G = lat.download_gt()
         U = lat.download_links()
     assert rep.final_residue <= 1e-15
-    # the fast path stops at the first half-sweep below the tolerance (the oracle on
-    # the reference schedule later), so its G agrees to what e2 ~ 1e-15 pins down
-    atol = 1e-12 if precision == gfc.PREC_FP64_EXACT else 1e-6
-    np.testing.assert_allclose(_mats(G), _mats(Gf) @ _mats(G0), atol=atol)
+    # the fast paths stop at the first half-sweep below the tolerance (the oracle on
+    # the reference schedule later), so their G agrees to what e2 ~ 1e-15 pins down;
+    # the FP32 phase of the mixed path also drifts along the residual gauge freedom
+    # (a rotation constant on each timeslice), which is removed before comparing
+    G_expect = (_mats(Gf) @ _mats(G0)).reshape(-1, 9)
+    G_expect = np.stack([G_expect.real, G_expect.imag], -1).reshape(-1)
+    if precision == gfc.PREC_MIXED:
+        res, drift = global_rotation_residual(G, G_expect, np.arange(ns ** 3 * nt) // ns ** 3)
+        print(f"mixed warm start: |G - h(t) G_ref| <= {res:.1e}, |h(t) - 1| <= {drift:.1e}")
+        assert res <= 1e-6
+    else:
+        atol = 1e-12 if precision == gfc.PREC_FP64_EXACT else 1e-6
+        np.testing.assert_allclose(_mats(G), _mats(Gf) @ _mats(G0), atol=atol)
     assert rep.functional == pytest.approx(orc.functional(U1, ns, nt), rel=1e-12)
     U2 = U0.copy()
     orc.apply_gt(U2, G, ns, nt)
@@ -154,11 +165,14 @@ def test_warm_start(precision, stop):
         assert orc.sha(U.reshape(-1, 4, 18)[:, 1:4, :]) == orc.sha(U1.reshape(-1, 4, 18)[:, 1:4, :])
 
 
-def test_warm_start_refused_on_the_mixed_path():
-    with gfc.Lattice(4, 4, mixed=True) as lat:
+@pytest.mark.parametrize("warm", [0, 1])
+def test_mixed_needs_a_mixed_context(warm):
+    """A context created without GFC_CTX_MIXED has no FP32 fields and no FP64 copy of
+    the start: the mixed path is refused with a message, cold or warm."""
+    with gfc.Lattice(4, 4) as lat:
         lat.upload_links(gfc.synth_config(4, 4, 135, 0.5), 8, False)
-        with pytest.raises(gfc.GFCError):
-            lat.fix(gfc.default_params(), gfc.options(precision=gfc.PREC_MIXED, warm_start=1))
+        with pytest.raises(gfc.GFCError, match="GFC_CTX_MIXED"):
+            lat.fix(gfc.default_params(), gfc.options(precision=gfc.PREC_MIXED, warm_start=warm))
 
 
 @pytest.mark.parametrize("elem_bytes,swap", [(8, True), (4, True), (8, False)])
@@ -205,8 +219,9 @@ def test_async_gt_download_matches_the_synchronous_one(elem_bytes, swap):
 
 
 def test_device_code_is_sm100a():
-    """The kernels the runtime loaded for this library are sm_100a machine code
-    (cudaFuncGetAttributes through the C ABI), with no PTX left for JIT."""
+    """The kernels the runtime loaded for this library are sm_100 machine code
+    compiled from the compute_100 virtual architecture (cudaFuncGetAttributes through
+    the C ABI); the library embeds nothing else (its build recipe names
+    arch=compute_100a,code=sm_100a only)."""
     binary, ptx = gfc.device_code_version(0)
-    assert binary == 100, (binary, ptx)
-    assert ptx == 0, (binary, ptx)
+    assert (binary, ptx) == (100, 100)

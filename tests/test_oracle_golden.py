@@ -82,3 +82,14 @@ def test_oracle_invariants(cases):
     # against |div A| ~ sqrt(e2) ~ 1.7e-12 that moves e2 by ~1e-4 relative.
     assert orc.e2(U1, ns, nt) == pytest.approx(final, rel=1e-3)
     np.testing.assert_allclose(U1, U, atol=1e-13)
+
+
+def test_generator_pinned_full_size():
+    """The 32^3x64 workload file (seed 2, H scale 0.5, big-endian FP64) the
+    reference's full-size fix was recorded on: both generators still make it."""
+    import json
+
+    c = {x["name"]: x for x in json.load(open(os.path.join(GOLDEN, "full_cases.json")))}["cfg1_32x64"]
+    for gen in (gfc.synth_config, orc.synth_config):
+        U = gen(c["ns"], c["nt"], c["seed"], c["scale"])
+        assert orc.sha(U.astype(">f8")) == c["cfg_sha256"], gen.__module__
