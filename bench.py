@@ -64,6 +64,9 @@ def parse_args():
                    help="exact,fp64,fp32 launch-shape indices to use instead of autotuning (to profile the "
                         "shapes the autotuner picks when no profiler slows its trial launches)")
     p.add_argument("--only", default="", help="comma list of batch,serve: run just those (no headline line)")
+    p.add_argument("--batch-shape", default="",
+                   help="minb32,minb64,round_sweeps of the batch sweeps instead of autotuning (to profile a "
+                        "fixed shape)")
     return p.parse_args()
 
 
@@ -347,6 +350,24 @@ def run_extras(a, lat, params, stream, torch, gfc, half):
                         vs_reference_golden=vs_golden(gold, rep, psm, ptm, ps0, pt0))
     res["mixed_speedup_vs_fp64_fast"] = rep64.seconds_total / rep.seconds_total
     res["mixed_speedup_vs_fp64_full"] = repf.seconds_total / rep.seconds_total
+    # the same with a later switch (e2 < 1e-11) and the FP32 links rebuilt from the
+    # FP64 start every 128 half-sweeps (options.fp32_refresh)
+    late = gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY, switch_e2=1e-11, fp32_refresh=128)
+    lat.restore_links()
+    lat.fix(params, late)   # warm
+    bestr = None
+    for _ in range(2):
+        lat.restore_links()
+        rcr, repr_ = lat.fix(params, late)
+        if bestr is None or repr_.seconds_total < bestr[1].seconds_total:
+            bestr = (rcr, repr_)
+    rcr, repr_ = bestr
+    psr, ptr = lat.plaquette()
+    res["mixed_refresh"] = dict(seconds=repr_.seconds_total, sweeps=rcr, sweeps_fp32=repr_.sweeps_fp32,
+                                switch_e2=1e-11, fp32_refresh=128, final_e2=repr_.final_residue,
+                                functional=repr_.functional, plaq_drift=max(abs(psr - ps0), abs(ptr - pt0)),
+                                vs_reference_golden=vs_golden(gold, repr_, psr, ptr, ps0, pt0))
+    res["mixed_refresh_speedup_vs_fp64_fast"] = rep64.seconds_total / repr_.seconds_total
     # isolated kernel timings (no fused reduction, no stopping test)
     lat.restore_links()
     res["kernel_fp64_fast_s"] = timed_halfsweeps(lat, stream, torch, 64, gfc.PREC_FP64_FAST)
@@ -460,7 +481,11 @@ def run_batch(a, gfc, torch, precision, rk=None):
     try:
         # launch shapes timed on the size that carries most of the work (one-time setup)
         t0 = time.perf_counter()
-        tune = b.autotune(*big)
+        if a.batch_shape:
+            b.set_shape(*[int(x) for x in a.batch_shape.split(",")])
+            tune = None
+        else:
+            tune = b.autotune(*big)
         t_tune = time.perf_counter() - t0
         stream = torch.cuda.ExternalStream(b.stream)
         slots = []

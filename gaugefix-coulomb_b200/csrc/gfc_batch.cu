@@ -260,13 +260,84 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
 // the slowest of several warps, and the item's e2 partials are summed over its
 // pieces per lane, then across the warp, in a fixed order.  Each thread stages into
 // and reads back from its own shared-memory slots only, so no CTA barrier is needed.
+// One work item of k_bsweep_w / k_bsweep_wf: its BCHUNK sites in pieces of 32.
+template <class S>
+__device__ __forceinline__ void bsweep_item_w(const BState &b, int2 item, unsigned char *stage) {
+    using T = typename S::T;
+    constexpr bool F64 = sizeof(T) == 8;
+    const int lane = threadIdx.x;
+    const int expect = F64 ? SS_FP64 : SS_FP32;
+    const int gid = item.x, chunk = item.y;
+    const int st = *(volatile int *)&b.state[gid];
+    const bool verify = F64 && st == SS_VERIFY;
+    if (st != expect && !verify) return;   // retired earlier in this round (uniform)
+    const int par = b.sweeps[gid] & 1;
+    const int track = verify ? 1 : (b.mflag[gid] & MF_NOW);
+    const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
+    const BSlot &sl = b.slots[slot];
+    const Lat &l = sl.l;
+    typename S::V *u, *g;
+    slot_fields<S>(sl, u, g);
+    const uint32_t vsh = l.vs >> 1;
+    double pre = 0.0, post = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < BCHUNK / 32; q++) {
+        const uint32_t off = (uint32_t)chunk * BCHUNK + (uint32_t)q * 32 + lane;
+        if (off >= vsh) break;
+        double a = 0.0, z = 0.0;
+        if (verify)
+            a = measure_site<S>(u, l, par, (uint32_t)t * vsh + off);
+        else
+            fast_site_staged<S, 32, false>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, track, a, z,
+                                           (typename S::V *)stage);
+        pre += a;
+        post += z;
+    }
+    if (track) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            pre += __shfl_down_sync(0xffffffffu, pre, o);
+            post += __shfl_down_sync(0xffffffffu, post, o);
+        }
+        if (lane == 0) {
+            double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
+            pp[0] = pre;
+            pp[1] = post;
+        }
+    }
+}
+
+// Both precisions in one persistent launch of one-warp CTAs: the FP32 items first,
+// then the FP64 ones, from one cursor, so a half-sweep has one tail instead of one
+// per precision and one launch fewer.  A thread's staging slots are the same column
+// of the shared array in both precisions' layouts.
+template <int MINB>
+__global__ void __launch_bounds__(32, MINB) k_bsweep_wf(BState b) {
+    extern __shared__ __align__(16) unsigned char bstage[];
+    const int n32 = b.counts[0], n = n32 + b.counts[1];
+    int *cursor = b.counts + 6;
+    const int lane = threadIdx.x;
+    // the previous half-sweep's reunitarisation flags have been consumed
+    if (blockIdx.x == 0 && lane == 0) b.counts[8] = b.counts[9] = 0;
+    int it = 0;
+    if (lane == 0) it = atomicAdd(cursor, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    while (it < n) {
+        int ahead = 0;
+        if (lane == 0) ahead = atomicAdd(cursor, 1);
+        if (it < n32)
+            bsweep_item_w<S32>(b, b.items32[it], bstage);
+        else
+            bsweep_item_w<S64R>(b, b.items64[it - n32], bstage);
+        it = __shfl_sync(0xffffffffu, ahead, 0);
+    }
+}
+
 template <class S, int MINB>
 __global__ void __launch_bounds__(32, MINB) k_bsweep_w(BState b) {
     extern __shared__ __align__(16) unsigned char bstage[];
-    using T = typename S::T;
-    constexpr bool F64 = sizeof(T) == 8;
+    constexpr bool F64 = sizeof(typename S::T) == 8;
     const int n = b.counts[F64 ? 1 : 0];
-    const int expect = F64 ? SS_FP64 : SS_FP32;
     const int2 *items = F64 ? b.items64 : b.items32;
     int *cursor = b.counts + (F64 ? 7 : 6);
     const int lane = threadIdx.x;
@@ -279,46 +350,7 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_w(BState b) {
         // the next item is requested while this one is swept
         int ahead = 0;
         if (lane == 0) ahead = atomicAdd(cursor, 1);
-        const int2 item = items[it];
-        const int gid = item.x, chunk = item.y;
-        const int st = *(volatile int *)&b.state[gid];
-        const bool verify = F64 && st == SS_VERIFY;
-        if (st == expect || verify) {
-            const int par = b.sweeps[gid] & 1;
-            const int track = verify ? 1 : (b.mflag[gid] & MF_NOW);
-            const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
-            const BSlot &sl = b.slots[slot];
-            const Lat &l = sl.l;
-            typename S::V *u, *g;
-            slot_fields<S>(sl, u, g);
-            const uint32_t vsh = l.vs >> 1;
-            double pre = 0.0, post = 0.0;
-#pragma unroll 1
-            for (int q = 0; q < BCHUNK / 32; q++) {
-                const uint32_t off = (uint32_t)chunk * BCHUNK + (uint32_t)q * 32 + lane;
-                if (off >= vsh) break;
-                double a = 0.0, z = 0.0;
-                if (verify)
-                    a = measure_site<S>(u, l, par, (uint32_t)t * vsh + off);
-                else
-                    fast_site_staged<S, 32, false>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, track,
-                                                   a, z, (typename S::V *)bstage);
-                pre += a;
-                post += z;
-            }
-            if (track) {
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    pre += __shfl_down_sync(0xffffffffu, pre, o);
-                    post += __shfl_down_sync(0xffffffffu, post, o);
-                }
-                if (lane == 0) {
-                    double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
-                    pp[0] = pre;
-                    pp[1] = post;
-                }
-            }
-        }
+        bsweep_item_w<S>(b, items[it], bstage);
         it = __shfl_sync(0xffffffffu, ahead, 0);
     }
 }
@@ -331,6 +363,13 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_w(BState b) {
 // threshold, FP64 -> done at the tolerance, NaN -> done with the status bit.
 __global__ void k_bslice(BState b) {
     const int lane = threadIdx.x & 31;
+    // both sweep kernels of this half-sweep have finished: count it and reset their
+    // item cursors for the next one
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        b.counts[4] += 1;
+        b.counts[6] = 0;
+        b.counts[7] = 0;
+    }
     for (int gid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gid < b.nslices;
          gid += (gridDim.x * blockDim.x) >> 5) {
         const int st = b.state[gid];
@@ -412,23 +451,13 @@ __global__ void k_bslice(BState b) {
     }
 }
 
-__global__ void k_btick(BState b) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        b.counts[4] += 1;
-        b.counts[6] = 0;   // item cursors of the next half-sweep
-        b.counts[7] = 0;
-    }
-}
-
 // projectSU3 of a timeslice's working fields after every `period` of its own
 // half-sweeps (its own count, so a lattice admitted later is treated exactly as if
-// it were alone)
+// it were alone); the FP32 or the FP64 timeslices, by S
 template <class S>
-__global__ void __launch_bounds__(BCHUNK) k_breunit(BState b, unsigned period) {
+__device__ __forceinline__ void breunit_part(const BState &b, unsigned period, int *due, int &ndue) {
     constexpr bool F64 = sizeof(typename S::T) == 8;
-    if (period == 0 || !b.counts[F64 ? 9 : 8]) return;   // no timeslice is due this half-sweep
-    __shared__ int due[BCHUNK];
-    __shared__ int ndue;
+    if (period == 0 || !b.counts[F64 ? 9 : 8]) return;   // none is due this half-sweep (uniform)
     const int n = b.counts[F64 ? 1 : 0];
     const int2 *items = F64 ? b.items64 : b.items32;
     const int expect = F64 ? SS_FP64 : SS_FP32;
@@ -468,6 +497,13 @@ __global__ void __launch_bounds__(BCHUNK) k_breunit(BState b, unsigned period) {
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(BCHUNK) k_breunit(BState b) {
+    __shared__ int due[BCHUNK];
+    __shared__ int ndue;
+    breunit_part<S32>(b, b.reunit32, due, ndue);
+    breunit_part<S64R>(b, b.reunit64, due, ndue);
 }
 
 // --------------------------------------------------- FP32 -> FP64 switch --
@@ -948,6 +984,24 @@ static void launch_bsweep_k(int grid, cudaStream_t st, const BState &bs) {
     kern<<<grid, BCHUNK, bytes, st>>>(bs);
 }
 
+template <int MINB>
+static void launch_bsweep_wf_k(int grid, cudaStream_t st, const BState &bs) {
+    constexpr size_t bytes = (size_t)6 * S64R::NS * 32 * 16;   // the larger of the two layouts
+    auto kern = k_bsweep_wf<MINB>;
+    static std::atomic<unsigned long long> done{0};
+    smem_attr_once(done, kern, bytes);
+    kern<<<grid, 32, bytes, st>>>(bs);
+}
+
+// both precisions in one launch of one-warp CTAs, minb (8, 11 or 12) per SM
+static void launch_bsweep_fused(int minb, int grid, cudaStream_t st, const BState &bs) {
+    switch (minb) {
+        case 8: return launch_bsweep_wf_k<8>(grid, st, bs);
+        case 12: return launch_bsweep_wf_k<12>(grid, st, bs);
+        default: return launch_bsweep_wf_k<11>(grid, st, bs);
+    }
+}
+
 template <class S, int MINB>
 static void launch_bsweep_w(int grid, cudaStream_t st, const BState &bs) {
     constexpr size_t bytes = (size_t)6 * S::NS * 32 * 16;
@@ -995,13 +1049,16 @@ static void enqueue_round(gfc_batch *b, const BState &bs) {
     for (int k = 0; k < b->round_k; k++) {
         // one resident wave of persistent CTAs: a CTA that had to wait for a slot
         // would start its share of the items late and stretch the tail
-        const int m64 = b->stage64 && b->minb64 <= 4 ? std::min(b->minb64, 3) : b->minb64;
-        launch_bsweep<S32>(b->minb32, false, b->nsm * b->minb32, st, bs);
-        launch_bsweep<S64R>(m64, b->stage64 != 0, b->nsm * m64, st, bs);
+        if (b->minb32 > 4 && b->minb64 > 4) {
+            // one-warp CTAs for both precisions: one launch, the FP64 shape
+            launch_bsweep_fused(b->minb64, b->nsm * b->minb64, st, bs);
+        } else {
+            const int m64 = b->stage64 && b->minb64 <= 4 ? std::min(b->minb64, 3) : b->minb64;
+            launch_bsweep<S32>(b->minb32, false, b->nsm * b->minb32, st, bs);
+            launch_bsweep<S64R>(m64, b->stage64 != 0, b->nsm * m64, st, bs);
+        }
         k_bslice<<<(b->nslices + 7) / 8, 256, 0, st>>>(bs);
-        k_btick<<<1, 32, 0, st>>>(bs);
-        k_breunit<S32><<<b->grid, BCHUNK, 0, st>>>(bs, bs.reunit32);
-        k_breunit<S64R><<<b->grid, BCHUNK, 0, st>>>(bs, bs.reunit64);
+        k_breunit<<<b->grid, BCHUNK, 0, st>>>(bs);
     }
 }
 
@@ -1038,7 +1095,7 @@ extern "C" int gfc_batch_round(gfc_batch *b, const gfc_params *p, const gfc_opti
     int rc = ensure_graph(b, p, o);
     if (rc) return rc;
     GFC_CHECK(cudaGraphLaunch(b->exec, b->s));
-    b->launches += 4 + 6 * b->round_k;
+    b->launches += 4 + (b->minb32 > 4 && b->minb64 > 4 ? 3 : 4) * b->round_k;
     b->rounds++;
     GFC_CHECK(cudaMemcpyAsync(b->hcounts, b->counts, sizeof(int) * 8, cudaMemcpyDeviceToHost, b->s));
     GFC_CHECK(cudaMemcpyAsync(b->hstate, b->state, sizeof(int) * b->nslices, cudaMemcpyDeviceToHost, b->s));
@@ -1321,7 +1378,9 @@ extern "C" int gfc_batch_autotune(gfc_batch *b, int ns, int nt, double *times) {
         double best = 1e30;
         const int m32[6] = {2, 3, 4, 8, 11, 12}, i32[6] = {0, 1, 2, 11, 12, 13};
         for (int q = 0; q < 6 && !rc; q++) {
-            gfc_batch_set_shape(b, m32[q], save64, 4);
+            // one-warp FP32 CTAs run in the launch they share with the FP64 items
+            // (k_bsweep_wf), whose shape is the FP64 one: time them in that shape
+            gfc_batch_set_shape(b, m32[q], m32[q] > 4 ? m32[q] : (save64 > 4 ? 3 : save64), 4);
             rc = time_rounds(GFC_PREC_MIXED, t[i32[q]]);
             if (!rc && t[i32[q]] < best) best = t[i32[q]], best32 = m32[q];
         }

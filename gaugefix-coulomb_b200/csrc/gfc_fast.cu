@@ -387,7 +387,7 @@ static void launch_shape(dim3 grid, cudaStream_t st, typename S::V *u, typename 
 
 template <class S>
 static constexpr size_t staged_bytes(int block, int sg, int nst) {
-    return (size_t)(nst + sg) * S::NS * block * 16;
+    return (size_t)(nst + sg) * S::NS * block * sizeof(typename S::V);
 }
 
 template <class S, int K>
@@ -766,16 +766,14 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     // start kept the links as uploaded, before G0 was applied, in u0 already)
     if (!o->warm_start)
         GFC_CHECK(cudaMemcpyAsync(c->u0, c->u, 3 * mat * sizeof(double2), cudaMemcpyDeviceToDevice, c->s));
-    {
-        dim3 gu((l.vh + 255) / 256, 3 * l.npar), gg((l.vh + 255) / 256, l.npar);
-        k_to_f32<<<gu, 256, 0, c->s>>>(c->u, (float4 *)c->u32, l.vh, 3 * l.npar);
-        k_identity32<<<gg, 256, 0, c->s>>>((float4 *)c->g32, l.vh, l.npar);
-        c->launches += 2;
-    }
-    // FP32 bulk, in pieces of fp32_refresh half-sweeps when refreshing
-    const unsigned reunit32 = std::min<unsigned>(p->sweeps_to_reunitarization, 50u);
+    const dim3 gu((l.vh + 255) / 256, 3 * l.npar), gg((l.vh + 255) / 256, l.npar);
     const int maxs = (int)p->max_sweeps_to_fix, K = o->fp32_refresh > 0 ? o->fp32_refresh : 0;
     int done = 0, below = -1;
+    k_to_f32<<<gu, 256, 0, c->s>>>(c->u, (float4 *)c->u32, l.vh, 3 * l.npar);
+    k_identity32<<<gg, 256, 0, c->s>>>((float4 *)c->g32, l.vh, l.npar);
+    c->launches += 2;
+    // FP32 bulk, in pieces of fp32_refresh half-sweeps when refreshing
+    const unsigned reunit32 = std::min<unsigned>(p->sweeps_to_reunitarization, 50u);
     for (;;) {
         const int lim = K ? std::min(maxs, done + K) : maxs;
         int d = done;
@@ -787,7 +785,6 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
         // refresh: G = G32 G in FP64 (projected), links G U0 G^dagger in FP64, rounded
         // to FP32 again; the FP32 G restarts from the identity
         if ((rc = ensure_2row(c))) return rc;
-        dim3 gg((l.vh + 255) / 256, l.npar), gu((l.vh + 255) / 256, 3 * l.npar);
         k_to_f64<<<gg, 256, 0, c->s>>>((const float4 *)c->g32, c->u64r, l.vh, l.npar);
         k_left_mul_gt<<<gg, 256, 0, c->s>>>(c->u64r, c->g, l.vh, l.npar);
         launch_apply_gt_spatial(c->u, c->u0, c->g, l, c->s);
@@ -804,7 +801,6 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     // switch: G in FP64 (rebuilt and projected), U = G U0 G^dagger from the FP64 start
     if ((rc = ensure_2row(c))) return rc;
     {
-        dim3 gg((l.vh + 255) / 256, l.npar);
         if (o->warm_start || K) {
             // G = G1 G0: G1 of the FP32 phase (FP64, in the two-row buffer, which
             // is free until the refinement) times the starting G0 (a warm start's,

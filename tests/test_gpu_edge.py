@@ -1,6 +1,8 @@
 """Edge lattices on the GPU: the smallest extents (ns = 2, where a site's forward and
-backward neighbours coincide), a single timeslice (nt = 1, the temporal link
-closes on its own site) and odd nt, on the exact, fast, mixed and batch paths."""
+backward neighbours coincide; ns = 1), a single timeslice (nt = 1, the temporal
+link closes on its own site), odd nt, and odd ns (7, 9: sites swept in parallel by
+boundary level, which must give the oracle's sequential z, y, x order bit for bit),
+on the exact, fast, mixed and batch paths."""
 import numpy as np
 import pytest
 
@@ -23,7 +25,7 @@ def unfixed(ns, nt, seed):
     return U
 
 
-@pytest.mark.parametrize("ns,nt", [(2, 1), (4, 1), (2, 3), (6, 1)])
+@pytest.mark.parametrize("ns,nt", [(2, 1), (4, 1), (2, 3), (6, 1), (1, 4), (7, 5), (9, 6)])
 def test_exact_oracle_fix_bit_for_bit(ns, nt):
     """The reference-arithmetic fix with the reference schedule against the oracle."""
     U = unfixed(ns, nt, 61)
@@ -41,7 +43,7 @@ def test_exact_oracle_fix_bit_for_bit(ns, nt):
     assert orc.sha(Ug.reshape(-1, 4, 18)[:, 1:4, :]) == orc.sha(Uo.reshape(-1, 4, 18)[:, 1:4, :])
 
 
-@pytest.mark.parametrize("ns,nt", [(2, 1), (4, 1), (2, 5), (6, 3)])
+@pytest.mark.parametrize("ns,nt", [(2, 1), (4, 1), (2, 5), (6, 3), (5, 4)])
 @pytest.mark.parametrize("prec", [gfc.PREC_FP64_FAST, gfc.PREC_MIXED, gfc.PREC_FP64_FULL])
 def test_fast_paths_on_edge_lattices(ns, nt, prec):
     U0 = unfixed(ns, nt, 62)

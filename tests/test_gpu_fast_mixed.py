@@ -186,3 +186,33 @@ def test_sparse_e2_measurement_stops_at_the_same_half_sweep(precision):
             out[dense] = (rc, rep.first_below_tol, rep.sweeps_fp32, orc.sha(lat.download_gt()))
             assert rep.final_residue <= 1e-15
     assert out[0] == out[1]
+
+
+@pytest.mark.parametrize("refresh,switch", [(64, 1e-11), (128, 1e-11), (16, 1e-10)])
+def test_mixed_with_fp32_refresh(refresh, switch):
+    """The mixed path with the FP32 links rebuilt from the FP64 start (as G U0 G^dagger
+    with the FP32 G folded into an FP64 G) every `refresh` half-sweeps: the result is
+    the fix the FP64 oracle gives (e2 below the tolerance, the same gauge functional,
+    G in SU(3), links G U0 G^dagger, plaquettes unchanged)."""
+    ns, nt, tol = 8, 8, 1e-15
+    U0 = gfc.synth_config(ns, nt, 58, 0.5)
+    orc.reunitarize(U0)
+    k_ref, Uref, Gref = first_below(ns, nt, U0, tol)
+    with gfc.Lattice(ns, nt, mixed=True) as lat:
+        lat.upload_links(U0, 8, False)
+        ps0, pt0 = lat.plaquette()
+        rc, rep = lat.fix(gfc.default_params(tolerance=tol),
+                          gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY, switch_e2=switch,
+                                      fp32_refresh=refresh))
+        ps1, pt1 = lat.plaquette()
+        G = lat.download_gt()
+        U = lat.download_links()
+        e2, _ = lat.e2_theta()
+    assert rc > 0 and 0 < rep.sweeps_fp32 < rc
+    assert e2 <= tol and rep.final_residue <= tol
+    assert su3_error(G) < 1e-13
+    assert abs(ps1 - ps0) < 1e-13 and abs(pt1 - pt0) < 1e-13
+    U1 = U0.copy()
+    orc.apply_gt(U1, G, ns, nt)
+    np.testing.assert_allclose(U1, U, atol=1e-12)
+    assert rep.functional == pytest.approx(orc.functional(Uref, ns, nt), rel=1e-10)
