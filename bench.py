@@ -58,6 +58,9 @@ def parse_args():
     p.add_argument("--no-precision-form", action="store_true", help="skip the 48^3x96 FP32-input mixed run")
     p.add_argument("--serve-requests", type=int, default=24, help="requests of the serving run (0: skip)")
     p.add_argument("--serve-rate", type=float, default=20.0, help="mean request arrival rate per second")
+    p.add_argument("--serve-sustained-rate", type=float, default=0.8,
+                   help="arrival rate of the second serving run, below what one B200 completes (0: skip)")
+    p.add_argument("--serve-sustained-requests", type=int, default=16)
     p.add_argument("--batch-mix", default="16x32:32,24x48:32,32x64:32",
                    help="batch run: comma list of NSxNT:count (default: the 96-config mix)")
     p.add_argument("--shapes", default="",
@@ -311,6 +314,8 @@ def run_extras(a, lat, params, stream, torch, gfc, half):
     res["fp64_exact_reference_schedule"] = dict(
         seconds=time.perf_counter() - t0, sweeps=rc, final_e2=rep.final_residue,
         site_updates_per_s=rep.sweeps * half / rep.seconds_sweeps,
+        seconds_per_half_sweep=rep.seconds_sweeps / rep.sweeps,
+        alg_gb_per_s=half * BYTES_PER_SITE_UPDATE["fp64_full"] * rep.sweeps / rep.seconds_sweeps / 1e9,
         g_bit_identical_to_reference=(None if gold is None else
                                       hashlib.sha256(lat.download_gt().tobytes()).hexdigest() == gold["gt_sha256"]),
         reference_half_sweeps=None if gold is None else gold["sweeps"])
@@ -371,8 +376,12 @@ def run_extras(a, lat, params, stream, torch, gfc, half):
     # isolated kernel timings (no fused reduction, no stopping test)
     lat.restore_links()
     res["kernel_fp64_fast_s"] = timed_halfsweeps(lat, stream, torch, 64, gfc.PREC_FP64_FAST)
+    # the exact half-sweep averaged over a whole fix (the sweep loop of the
+    # reference-schedule fix above), and over the first 36 half-sweeps from the
+    # unfixed links alone, where the update's data-dependent branches diverge most
+    res["kernel_fp64_exact_s"] = res["fp64_exact_reference_schedule"]["seconds_per_half_sweep"]
     lat.restore_links()
-    res["kernel_fp64_exact_s"] = timed_halfsweeps(lat, stream, torch, 32, gfc.PREC_FP64_EXACT)
+    res["kernel_fp64_exact_unfixed_s"] = timed_halfsweeps(lat, stream, torch, 32, gfc.PREC_FP64_EXACT)
     lat.restore_links()
     return res
 
@@ -707,6 +716,9 @@ def main():
                                                       gfc.SERVE_ALL)
             elif m == "serve64":
                 out["serve_fp64"] = run_serve(a, gfc, gfc.PREC_FP64_FAST, a.serve_requests, a.serve_rate)
+            elif m == "serve_sustained":
+                out["serve_mixed_sustained"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_sustained_requests,
+                                                         a.serve_sustained_rate)
         if rk.rank == 0:
             print(json.dumps(out))
         rk.close()
@@ -727,6 +739,10 @@ def main():
             r["extras"]["serve_fp64"] = run_serve(a, gfc, gfc.PREC_FP64_FAST, a.serve_requests, a.serve_rate)
             r["extras"]["serve_mixed_shared"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate,
                                                           gfc.SERVE_ALL)
+        if a.serve_sustained_rate > 0 and a.serve_sustained_requests > 0:
+            # a stream the GPU keeps up with: latency is service time plus short queueing
+            r["extras"]["serve_mixed_sustained"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_sustained_requests,
+                                                             a.serve_sustained_rate)
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):

@@ -140,19 +140,18 @@ __device__ __forceinline__ double2 xcmul(double2 a, double2 b) {
 // |z| as glibc computes it: Borges, "An improved algorithm for hypot(a,b)" (2019),
 // the correction step without fused multiply-add, with power-of-two rescaling for
 // extreme exponents and the early exit for a negligible smaller operand.
+// Both correction forms are evaluated and one is selected: the sites of a warp take
+// either, so a branch would run both for the warp anyway.
 __device__ __forceinline__ double xhypot_kernel(double ax, double ay) {
-    double h = __dsqrt_rn(xa(xm(ax, ax), xm(ay, ay)));
-    double t1, t2;
-    if (h <= xm(2.0, ay)) {
-        double dl = xs(h, ay);
-        t1 = xm(ax, xs(xm(2.0, dl), ax));
-        t2 = xm(xs(dl, xm(2.0, xs(ax, ay))), dl);
-    } else {
-        double dl = xs(h, ax);
-        t1 = xm(xm(2.0, dl), xs(ax, xm(2.0, ay)));
-        t2 = xa(xm(xs(xm(4.0, dl), ay), ay), xm(dl, dl));
-    }
-    return xs(h, xd(xa(t1, t2), xm(2.0, h)));
+    const double h = __dsqrt_rn(xa(xm(ax, ax), xm(ay, ay)));
+    const double da = xs(h, ay);
+    const double t1a = xm(ax, xs(xm(2.0, da), ax));
+    const double t2a = xm(xs(da, xm(2.0, xs(ax, ay))), da);
+    const double db = xs(h, ax);
+    const double t1b = xm(xm(2.0, db), xs(ax, xm(2.0, ay)));
+    const double t2b = xa(xm(xs(xm(4.0, db), ay), ay), xm(db, db));
+    const bool a = h <= xm(2.0, ay);
+    return xs(h, xd(xa(a ? t1a : t1b, a ? t2a : t2b), xm(2.0, h)));
 }
 __device__ __forceinline__ double xhypot(double x, double y) {
     double ax = fabs(x), ay = fabs(y);
@@ -205,31 +204,35 @@ __device__ __forceinline__ void xprod_dag(const M3 &a, const M3 &b, M3 &c) {
 
 // Smith division of every entry of num by the same complex d (inverse3x3's
 // "/ a_det", SU3_ops.c:843-900); ratio and denominator do not depend on the entry.
+// The two cases (|Re d| < |Im d| or not) differ only in which operands enter the
+// same sequence of rounded operations, so the operands are selected instead of
+// branched on: sites of one warp take different cases, and a branch would run the
+// divisions of both for the whole warp.  The results are those of the branches.
 struct SmithDen {
     double r, den;
     int c_ge_d, tiny;
 };
 __device__ __forceinline__ SmithDen smith_prepare(double2 dd) {
     SmithDen s;
-    double c = dd.x, d = dd.y;
+    const double c = dd.x, d = dd.y;
     s.c_ge_d = !(fabs(c) < fabs(d));
-    if (!s.c_ge_d) {
-        s.r = xd(c, d);
-        s.den = xa(xm(c, s.r), d);
-    } else {
-        s.r = xd(d, c);
-        s.den = xa(xm(d, s.r), c);
-    }
+    const double num = s.c_ge_d ? d : c, dnm = s.c_ge_d ? c : d;   // r = d/c or c/d
+    s.r = xd(num, dnm);
+    s.den = xa(xm(num, s.r), dnm);                                   // d r + c or c r + d
     s.tiny = !(fabs(s.r) > 2.2250738585072014e-308);
     return s;
 }
 __device__ __forceinline__ double2 smith_div(double2 x, double2 dd, const SmithDen &s) {
-    double a = x.x, b = x.y, c = dd.x, d = dd.y;
-    if (!s.c_ge_d) {
-        if (!s.tiny) return make_double2(xd(xa(xm(a, s.r), b), s.den), xd(xs(xm(b, s.r), a), s.den));
-        return make_double2(xd(xa(xm(c, xd(a, d)), b), s.den), xd(xs(xm(c, xd(b, d)), a), s.den));
+    const double a = x.x, b = x.y, c = dd.x, d = dd.y;
+    if (!s.tiny) {
+        // c >= d: re = (b r + a) / den, im = (b - a r) / den
+        // c <  d: re = (a r + b) / den, im = (b r - a) / den
+        const double p = s.c_ge_d ? b : a, q = s.c_ge_d ? a : b;
+        const double t = xm(q, s.r);
+        const double hi = s.c_ge_d ? b : t, lo = s.c_ge_d ? t : a;
+        return make_double2(xd(xa(xm(p, s.r), q), s.den), xd(xs(hi, lo), s.den));
     }
-    if (!s.tiny) return make_double2(xd(xa(xm(b, s.r), a), s.den), xd(xs(b, xm(a, s.r)), s.den));
+    if (!s.c_ge_d) return make_double2(xd(xa(xm(c, xd(a, d)), b), s.den), xd(xs(xm(c, xd(b, d)), a), s.den));
     return make_double2(xd(xa(a, xm(d, xd(b, c))), s.den), xd(xs(b, xm(d, xd(a, c))), s.den));
 }
 

@@ -850,7 +850,7 @@ extern "C" int gfc_ctx_autotune(gfc_ctx *c, int which, double *times_out) {
     double times[GFC_TUNE_SLOTS] = {0.0};
     if (times_out)
         for (int k = 0; k < GFC_TUNE_SLOTS; k++) times_out[k] = 0.0;
-    if (!c->lat.cb) return GFC_OK;   // odd ns: one serial kernel, nothing to choose
+    if (!c->lat.cb) return GFC_OK;   // odd ns: one kernel (boundary levels), nothing to choose
     GFC_CHECK(cudaSetDevice(c->dev));
     int rc = gfc_ctx_save_links(c);
     if (rc) return rc;

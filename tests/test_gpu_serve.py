@@ -84,3 +84,23 @@ def test_smallest_first_policy():
     assert t_small < t_big
     assert out[big].tobytes() == alone(8, 8, 121, 0.5, gfc.PREC_MIXED).tobytes()
     assert out[small].tobytes() == alone(4, 4, 122, 0.5, gfc.PREC_MIXED).tobytes()
+
+
+def test_larger_requests_admitted_while_others_run():
+    """Requests of 16^3x16 and 12^3x12 submitted while a 16^3x8 is being swept, in
+    both precisions: each G equals the lattice fixed alone, bit for bit."""
+    p = gfc.default_params(tolerance=TOL)
+    reqs = [(16, 8, 131, 0.6, gfc.PREC_MIXED), (16, 16, 132, 0.4, gfc.PREC_FP64_FAST),
+            (12, 12, 133, 0.7, gfc.PREC_MIXED)]
+    with gfc.Server(max_sites=2 * 10 ** 5, max_slots=4, max_nt=16) as srv:
+        first = srv.submit(*reqs[0][:2], seed=reqs[0][2], scale=reqs[0][3], precision=reqs[0][4])
+        for _ in range(3):
+            srv.step(p, gfc.options(precision=gfc.PREC_MIXED))
+        later = [srv.submit(ns, nt, seed=sd, scale=sc, precision=pr) for ns, nt, sd, sc, pr in reqs[1:]]
+        ids = [first] + later
+        out = run_until_done(srv, ids, p, gfc.options(precision=gfc.PREC_MIXED))
+        for rid in ids:
+            rep = srv.poll(rid)[3]
+            assert rep.status > 0 and rep.e2 <= TOL
+    for rid, (ns, nt, sd, sc, pr) in zip(ids, reqs):
+        assert out[rid].tobytes() == alone(ns, nt, sd, sc, pr).tobytes()
