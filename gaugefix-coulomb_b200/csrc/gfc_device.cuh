@@ -128,6 +128,8 @@ __device__ __forceinline__ double xm(double a, double b) { return __dmul_rn(a, b
 __device__ __forceinline__ double xa(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double xs(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double xd(double a, double b) { return __ddiv_rn(a, b); }
+// 1 / b correctly rounded: by IEEE round-to-nearest the same value as xd(1.0, b)
+__device__ __forceinline__ double xrcp(double b) { return __drcp_rn(b); }
 
 __device__ __forceinline__ double2 cz() { return make_double2(0.0, 0.0); }
 __device__ __forceinline__ double2 xcadd(double2 a, double2 b) { return make_double2(xa(a.x, b.x), xa(a.y, b.y)); }
@@ -278,7 +280,7 @@ __device__ __forceinline__ int xnormalize(double2 v[3]) {
         r = xa(r, xm(h, h));
     }
     if (r != 0.0) {
-        r = xd(1.0, __dsqrt_rn(r));
+        r = xrcp(__dsqrt_rn(r));
 #pragma unroll
         for (int a = 0; a < 3; a++) v[a] = make_double2(xm(v[a].x, r), xm(v[a].y, r));
         return 0;
@@ -325,7 +327,7 @@ __device__ __forceinline__ void xsub_los_alamos(M3 &w) {
     double k3 = -xs(m[EL(A, A)].y, m[EL(B, B)].y);
     double det = xa(xa(xa(xa(0.0, xm(k0, k0)), xm(k1, k1)), xm(k2, k2)), xm(k3, k3));
     if (det == 0.0) return;
-    double inv = xd(1.0, __dsqrt_rn(det));
+    double inv = xrcp(__dsqrt_rn(det));
     k0 = xm(inv, k0);
     k1 = xm(inv, k1);
     k2 = xm(inv, k2);

@@ -58,6 +58,26 @@ def test_exact_path_bit_for_bit(cases, tmp_path, name):
         # gauge-invariant value; ours stays equal to the value before (checked above).
 
 
+@pytest.mark.parametrize("name", ["l3x4_oddns", "l5x4_oddns"])
+@pytest.mark.parametrize("precision", [gfc.PREC_FP64_FAST, gfc.PREC_MIXED, gfc.PREC_FP64_FULL])
+def test_odd_ns_on_every_precision(cases, tmp_path, name, precision):
+    """Odd ns on the fast FP64, full FP64 and mixed options: same-parity sites meet
+    across the boundary there, and those options sweep odd ns with the boundary-level
+    kernel in the reference's arithmetic, so G and the spatial links are the
+    reference's bit for bit, after the same half-sweeps."""
+    c = cases[name]
+    ns, nt = c["ns"], c["nt"]
+    with gfc.Lattice(ns, nt, mixed=True) as lat:
+        lat.upload_links(raw_config(c), 8, byteswap=True)
+        lat.reunitarize()
+        rc, rep = lat.fix(case_params(c, tmp_path), gfc.options(precision=precision))
+        G = lat.download_gt()
+        U = lat.download_links()
+    assert rc == c["sweeps"]
+    assert orc.sha(G) == c["gt_sha256"]
+    assert orc.sha(U.reshape(-1, 4, 18)[:, 1:4, :]) == c["u_spatial_sha256"]
+
+
 @pytest.mark.parametrize("name", ["l4x8", "cfg0_8x16", "l4x8_maxsweeps"])
 def test_one_shot_entry_point(cases, tmp_path, name):
     """gfc_gaugefix_overrelaxation on host arrays, as the reference's main calls
