@@ -37,7 +37,14 @@
 
 namespace gfc {
 
-enum : int { SS_EMPTY = 0, SS_FP32 = 1, SS_PEND = 2, SS_FP64 = 3, SS_DONE = 4, SS_VERIFY = 5 };
+enum : int { SS_EMPTY = 0, SS_FP32 = 1, SS_PEND = 2, SS_FP64 = 3, SS_DONE = 4, SS_VERIFY = 5, SS_LEX = 6 };
+// SS_LEX: a timeslice of an odd-ns lattice, FP64 on two stored rows in the
+// lexicographic layout.  Same-parity sites meet across the periodic boundary there,
+// so a half-sweep runs as four launches over the boundary levels (the number of
+// coordinates equal to ns - 1), which keeps the order of the sequential z, y, x
+// sweep between every pair of sites that share a link; e2 is measured by a separate
+// pass over the state the half-sweep leaves (a site's post-update w is not final
+// when a later level updates a neighbour), so no verify pass is needed.
 // SS_VERIFY: the FP64 e2 measured after half-sweep c - 1 fell below the tolerance, but
 // the timeslice has had half-sweep c too.  Its next pass measures e2 of the state it
 // is in without updating it: below the tolerance -> DONE with that state, else back
@@ -74,10 +81,12 @@ struct BState {
     int *mk;              // [nslices] own half-sweep count of the last e2 measurement (-1: none)
     double *me2;          // [nslices] that e2
     double *ring;         // [2][nslices][2]: (pre, post) e2 sums of the last two half-sweeps
-    int2 *items32, *items64, *pend;
+    int2 *items32, *items64, *pend, *itemslex;
     int cap_items, cap_pend;
+    int lex;              // 1: odd-ns slots may be active (their launches are in the round)
     int *counts;          // [0] n32 [1] n64 [2] npend [3] active timeslices [4] half-sweep k [5] overflow
                           // [6] [7] item cursors [8] [9] FP32 / FP64 reunitarisation due
+                          // [10] nlex [11..14] cursors of the odd-ns levels [15] of the odd-ns e2 pass
     unsigned *status;
     double omega, switch_e2, tol;
     unsigned hits, reunit32, reunit64;
@@ -86,16 +95,16 @@ struct BState {
 // ------------------------------------------------------------------ compaction --
 // One block.  Builds the three work lists from the state table.
 __global__ void __launch_bounds__(1024) k_compact(BState b) {
-    __shared__ int sc[3][1024];
+    __shared__ int sc[4][1024];
     __shared__ int sact[1024];
     const int tid = threadIdx.x;
     const int per = (b.nslices + 1023) / 1024;
     const int g0 = tid * per, g1 = min(g0 + per, b.nslices);
-    int c[3] = {0, 0, 0}, act = 0;
+    int c[4] = {0, 0, 0, 0}, act = 0;
     for (int gid = g0; gid < g1; gid++) {
         int st = b.state[gid];
         const bool held = b.held[gid / b.max_nt];
-        b.listed[gid] = !held && (st == SS_FP32 || st == SS_FP64 || st == SS_VERIFY);
+        b.listed[gid] = !held && (st == SS_FP32 || st == SS_FP64 || st == SS_VERIFY || st == SS_LEX);
         if (st == SS_EMPTY || st == SS_DONE) continue;
         const BSlot &sl = b.slots[gid / b.max_nt];
         act++;
@@ -103,22 +112,23 @@ __global__ void __launch_bounds__(1024) k_compact(BState b) {
         if (st == SS_FP32) c[0] += sl.nbx;
         else if (st == SS_FP64 || st == SS_VERIFY) c[1] += sl.nbx;
         else if (st == SS_PEND) c[2] += sl.nfull;
+        else if (st == SS_LEX) c[3] += sl.nbx;
     }
-    for (int q = 0; q < 3; q++) sc[q][tid] = c[q];
+    for (int q = 0; q < 4; q++) sc[q][tid] = c[q];
     sact[tid] = act;
     __syncthreads();
     // inclusive Hillis-Steele scans
     for (int off = 1; off < 1024; off <<= 1) {
-        int v[3], a = 0;
-        for (int q = 0; q < 3; q++) v[q] = tid >= off ? sc[q][tid - off] : 0;
+        int v[4], a = 0;
+        for (int q = 0; q < 4; q++) v[q] = tid >= off ? sc[q][tid - off] : 0;
         if (tid >= off) a = sact[tid - off];
         __syncthreads();
-        for (int q = 0; q < 3; q++) sc[q][tid] += v[q];
+        for (int q = 0; q < 4; q++) sc[q][tid] += v[q];
         sact[tid] += a;
         __syncthreads();
     }
-    int o[3];
-    for (int q = 0; q < 3; q++) o[q] = sc[q][tid] - c[q];
+    int o[4];
+    for (int q = 0; q < 4; q++) o[q] = sc[q][tid] - c[q];
     int overflow = 0;
     for (int gid = g0; gid < g1; gid++) {
         int st = b.state[gid];
@@ -134,6 +144,10 @@ __global__ void __launch_bounds__(1024) k_compact(BState b) {
             for (int ch = 0; ch < sl.nfull; ch++, o[2]++)
                 if (o[2] < b.cap_pend) b.pend[o[2]] = make_int2(gid, ch);
                 else overflow = 1;
+        } else if (st == SS_LEX) {
+            for (int ch = 0; ch < sl.nbx; ch++, o[3]++)
+                if (o[3] < b.cap_pend) b.itemslex[o[3]] = make_int2(gid, ch);
+                else overflow = 1;
         }
     }
     if (overflow) atomicOr(&b.counts[5], 1);
@@ -144,6 +158,8 @@ __global__ void __launch_bounds__(1024) k_compact(BState b) {
         b.counts[3] = sact[1023];
         b.counts[6] = 0;
         b.counts[7] = 0;
+        b.counts[10] = min(sc[3][1023], b.cap_pend);
+        for (int q = 11; q < 16; q++) b.counts[q] = 0;
     }
 }
 
@@ -355,6 +371,79 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_w(BState b) {
     }
 }
 
+// Odd-ns timeslices, boundary level `level` of one half-sweep: one-warp CTAs take
+// 32-site pieces of the odd-ns work items (chunks of a timeslice in lexicographic
+// order); a lane updates its site if it has the half-sweep's parity and the level.
+// Sites of one level share no link, and every pair that does share one is in
+// consecutive levels in the sequential sweep's order (see SS_LEX).
+template <int MINB>
+__global__ void __launch_bounds__(32, MINB) k_bsweep_lex(BState b, int level) {
+    extern __shared__ __align__(16) unsigned char bstage[];
+    const int n = b.counts[10] * BPIECES;
+    int *cursor = b.counts + 11 + level;
+    const int lane = threadIdx.x;
+    int it = 0;
+    if (lane == 0) it = atomicAdd(cursor, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    while (it < n) {
+        int ahead = 0;
+        if (lane == 0) ahead = atomicAdd(cursor, 1);
+        const int2 item = b.itemslex[it / BPIECES];
+        const int gid = item.x;
+        if (*(volatile int *)&b.state[gid] == SS_LEX) {   // uniform in the CTA
+            const int par = b.sweeps[gid] & 1;
+            const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
+            const BSlot &sl = b.slots[slot];
+            const Lat &l = sl.l;
+            const uint32_t off = (uint32_t)item.y * BCHUNK + (uint32_t)(it % BPIECES) * 32 + lane;
+            if (off < l.vs) {
+                const uint32_t L = (uint32_t)t * l.vs + off;
+                const Coord c = coord_lex(l, L);
+                const uint32_t e = (uint32_t)l.ns - 1;
+                const int lev = (int)(c.x == e) + (int)(c.y == e) + (int)(c.z == e);
+                if ((int)((c.x + c.y + c.z + c.t) & 1u) == par && lev == level) {
+                    double a = 0.0, z = 0.0;
+                    fast_site_staged<S64R, 32, false, 6, false>(sl.u64r, sl.g64r, l, 0, L, b.omega, b.hits, 0, a, z,
+                                                                 (double2 *)bstage);
+                }
+            }
+        }
+        it = __shfl_sync(0xffffffffu, ahead, 0);
+    }
+}
+
+// e2 of the odd-ns timeslices measured on this half-sweep (mflag MF_NOW), over all
+// their sites, on the state the four level launches left: per-piece partials.
+__global__ void __launch_bounds__(32) k_bmeasure_lex(BState b) {
+    const int n = b.counts[10] * BPIECES;
+    int *cursor = b.counts + 15;
+    const int lane = threadIdx.x;
+    int it = 0;
+    if (lane == 0) it = atomicAdd(cursor, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    while (it < n) {
+        int ahead = 0;
+        if (lane == 0) ahead = atomicAdd(cursor, 1);
+        const int2 item = b.itemslex[it / BPIECES];
+        const int gid = item.x, q = it % BPIECES;
+        if (*(volatile int *)&b.state[gid] == SS_LEX && (b.mflag[gid] & MF_NOW)) {   // uniform in the CTA
+            const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
+            const BSlot &sl = b.slots[slot];
+            const Lat &l = sl.l;
+            const uint32_t off = (uint32_t)item.y * BCHUNK + (uint32_t)q * 32 + lane;
+            double v = off < l.vs ? measure_site<S64R, false>(sl.u64r, l, 0, (uint32_t)t * l.vs + off) : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) {
+                double *pp = sl.part + (((size_t)t * sl.nbx + item.y) * BPIECES + q) * 2;
+                pp[0] = v;
+                pp[1] = 0.0;
+            }
+        }
+        it = __shfl_sync(0xffffffffu, ahead, 0);
+    }
+}
+
 // After both sweep kernels of a half-sweep, one warp per swept timeslice: advances its
 // half-sweep count and e2 measurement schedule; where the half-sweep was measured,
 // sums the chunk partials in a fixed order (lane-strided, then a shuffle tree) and,
@@ -369,13 +458,15 @@ __global__ void k_bslice(BState b) {
         b.counts[4] += 1;
         b.counts[6] = 0;
         b.counts[7] = 0;
+        for (int q = 11; q < 16; q++) b.counts[q] = 0;
     }
     for (int gid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gid < b.nslices;
          gid += (gridDim.x * blockDim.x) >> 5) {
         const int st = b.state[gid];
         // swept in this half-sweep: listed at the round's start and not retired since
         // (a timeslice switched to FP64 at the start of the round has no items yet)
-        if (!b.listed[gid] || (st != SS_FP32 && st != SS_FP64 && st != SS_VERIFY)) continue;   // uniform in the warp
+        if (!b.listed[gid] || (st != SS_FP32 && st != SS_FP64 && st != SS_VERIFY && st != SS_LEX))
+            continue;   // uniform in the warp
         const int f = st == SS_VERIFY ? MF_NOW : b.mflag[gid];
         const int c = b.sweeps[gid];   // this half-sweep's own index
         const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
@@ -394,6 +485,34 @@ __global__ void k_bslice(BState b) {
             }
         }
         if (lane != 0) continue;
+        if (st == SS_LEX) {
+            // e2 of the state after this half-sweep, measured by k_bmeasure_lex
+            int nf = f & MF_DENSE, nst = st;
+            if (f & MF_NOW) {
+                const double e2s = s0 / (double)sl.l.vs;
+                if (!(s0 == s0)) {
+                    atomicOr(b.status, GFC_STATUS_NAN);
+                    nst = SS_DONE;
+                } else if (e2s <= b.tol) {
+                    nst = SS_DONE;
+                } else if (!(nf & MF_DENSE)) {
+                    if (e2s <= 1e3 * b.tol) {
+                        nf |= MF_DENSE;
+                    } else if (b.mk[gid] >= 0 && e2s < b.me2[gid]) {
+                        const double rate = pow(e2s / b.me2[gid], 1.0 / (double)(c - b.mk[gid]));
+                        if (e2s * pow(rate, 2.0 * MEASURE_PERIOD) <= 10.0 * b.tol) nf |= MF_DENSE;
+                    }
+                }
+                b.mk[gid] = c;
+                b.me2[gid] = e2s;
+            }
+            if ((nf & MF_DENSE) || measure_at(c + 1)) nf |= MF_NOW;
+            b.mflag[gid] = nf;
+            b.sweeps[gid] = c + 1;
+            if (nst != st) b.state[gid] = nst;
+            else if (b.reunit64 && (unsigned)(c + 1) % b.reunit64 == 0) b.counts[9] = 1;
+            continue;
+        }
         if (st == SS_VERIFY) {
             // measure-only pass: e2 of the current state = post of the last half-sweep
             // applied (index c - 1) + the other parity now; nothing was applied
@@ -455,12 +574,13 @@ __global__ void k_bslice(BState b) {
 // half-sweeps (its own count, so a lattice admitted later is treated exactly as if
 // it were alone); the FP32 or the FP64 timeslices, by S
 template <class S>
-__device__ __forceinline__ void breunit_part(const BState &b, unsigned period, int *due, int &ndue) {
+__device__ __forceinline__ void breunit_part(const BState &b, unsigned period, int *due, int &ndue,
+                                             bool lex = false) {
     constexpr bool F64 = sizeof(typename S::T) == 8;
     if (period == 0 || !b.counts[F64 ? 9 : 8]) return;   // none is due this half-sweep (uniform)
-    const int n = b.counts[F64 ? 1 : 0];
-    const int2 *items = F64 ? b.items64 : b.items32;
-    const int expect = F64 ? SS_FP64 : SS_FP32;
+    const int n = lex ? b.counts[10] : b.counts[F64 ? 1 : 0];
+    const int2 *items = lex ? b.itemslex : (F64 ? b.items64 : b.items32);
+    const int expect = lex ? SS_LEX : (F64 ? SS_FP64 : SS_FP32);
     // the CTA examines BCHUNK items at once (one per thread) and projects only the
     // chunks of timeslices that are due; most half-sweeps none are
     for (int base = blockIdx.x * BCHUNK; base < n; base += gridDim.x * BCHUNK) {
@@ -481,11 +601,11 @@ __device__ __forceinline__ void breunit_part(const BState &b, unsigned period, i
             const Lat l = sl.l;
             typename S::V *u, *g;
             slot_fields<S>(sl, u, g);
-            const uint32_t vsh = l.vs >> 1;
+            const uint32_t span = l.cb ? l.vs >> 1 : l.vs;   // sites of a timeslice per parity slot
             const uint32_t off = (uint32_t)item.y * BCHUNK + threadIdx.x;
-            if (off >= vsh) continue;
-            const uint32_t i = (uint32_t)t * vsh + off;
-            for (int par = 0; par < 2; par++) {
+            if (off >= span) continue;
+            const uint32_t i = (uint32_t)t * span + off;
+            for (int par = 0; par < l.npar; par++) {
                 for (int d = 0; d <= 3; d++) {
                     typename S::V *p = d < 3 ? u + su_idx<S>(l, d, par, i) : g + sg_idx<S>(l, par, i);
                     Mt<typename S::T> m;
@@ -504,6 +624,7 @@ __global__ void __launch_bounds__(BCHUNK) k_breunit(BState b) {
     __shared__ int ndue;
     breunit_part<S32>(b, b.reunit32, due, ndue);
     breunit_part<S64R>(b, b.reunit64, due, ndue);
+    if (b.lex) breunit_part<S64R>(b, b.reunit64, due, ndue, true);
 }
 
 // --------------------------------------------------- FP32 -> FP64 switch --
@@ -606,8 +727,9 @@ struct gfc_batch {
     int *state = nullptr, *sweeps = nullptr, *counts = nullptr, *listed = nullptr, *mflag = nullptr, *mk = nullptr;
     double *me2 = nullptr;
     double *ring = nullptr;
-    int2 *items32 = nullptr, *items64 = nullptr, *pend = nullptr;
+    int2 *items32 = nullptr, *items64 = nullptr, *pend = nullptr, *itemslex = nullptr;
     int cap_items = 0, cap_pend = 0;
+    int odd_slots = 0;               // slots of odd ns in use (their launches join the round)
     unsigned *status = nullptr;
     int *hcounts = nullptr;          // pinned mirror [8]
     int *hstate = nullptr;           // pinned mirror [nslices]
@@ -676,6 +798,7 @@ extern "C" int gfc_batch_create(int device, size_t max_sites, int max_slots, int
     BTRY(cudaMalloc(&b->items32, sizeof(int2) * b->cap_items));
     BTRY(cudaMalloc(&b->items64, sizeof(int2) * b->cap_items));
     BTRY(cudaMalloc(&b->pend, sizeof(int2) * b->cap_pend));
+    BTRY(cudaMalloc(&b->itemslex, sizeof(int2) * b->cap_pend));   // chunks over whole timeslices
     BTRY(cudaMalloc(&b->counts, sizeof(int) * 16));
     BTRY(cudaMemset(b->counts, 0, sizeof(int) * 16));
     BTRY(cudaMalloc(&b->status, sizeof(unsigned)));
@@ -729,6 +852,7 @@ extern "C" int gfc_batch_destroy(gfc_batch *b) {
     cudaFree(b->items32);
     cudaFree(b->items64);
     cudaFree(b->pend);
+    cudaFree(b->itemslex);
     cudaFree(b->counts);
     cudaFree(b->status);
     cudaFree(b->part);
@@ -742,21 +866,24 @@ extern "C" int gfc_batch_destroy(gfc_batch *b) {
 }
 
 // bytes of device memory one slot of ns^3 x nt needs
+// chunks of one timeslice's sites of one parity slot (odd ns: the whole timeslice)
+static size_t slot_chunks(const Lat &l) { return ((l.cb ? l.vs >> 1 : l.vs) + BCHUNK - 1) / BCHUNK; }
+
 extern "C" size_t gfc_batch_slot_bytes(int ns, int nt) {
     Lat l = make_lat(ns, nt);
-    size_t vh = l.vh;
-    size_t nbx = ((l.vs >> 1) + BCHUNK - 1) / BCHUNK;
-    return al256(3 * 2 * vh * 9 * 16) + 2 * al256(2 * vh * 9 * 16)            // u, ut, g
-           + al256(3 * 2 * vh * 6 * 16) + al256(2 * vh * 6 * 16)              // u64r, g64r
-           + al256(3 * 2 * vh * 3 * 16) + al256(2 * vh * 3 * 16)              // u32, g32
-           + al256((size_t)nt * nbx * BPIECES * 2 * 8) + 4096;  // piece partials
+    const size_t m = (size_t)l.npar * l.vh;   // matrices per field (V)
+    const size_t nbx = slot_chunks(l);
+    return al256(3 * m * 9 * 16) + 2 * al256(m * 9 * 16)            // u, ut, g
+           + al256(3 * m * 6 * 16) + al256(m * 6 * 16)              // u64r, g64r
+           + al256(3 * m * 3 * 16) + al256(m * 3 * 16)              // u32, g32
+           + al256((size_t)nt * nbx * BPIECES * 2 * 8) + 4096;      // piece partials
 }
 
 extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
     if (!b || !slot_out) return GFC_ERR_ARG;
     *slot_out = -1;
-    if (ns <= 0 || nt <= 0 || (ns & 1) || nt > b->max_nt) {
-        set_error("batch slots need even ns and nt <= %d (got %d, %d)", b->max_nt, ns, nt);
+    if (ns <= 0 || nt <= 0 || nt > b->max_nt) {
+        set_error("batch slots need ns > 0 and 0 < nt <= %d (got %d, %d)", b->max_nt, ns, nt);
         return GFC_ERR_GEOMETRY;
     }
     const size_t V = (size_t)ns * ns * ns * nt;
@@ -793,21 +920,21 @@ extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
     }
     BSlot sl{};
     sl.l = make_lat(ns, nt);
-    const size_t vh = sl.l.vh;
+    const size_t mv = (size_t)sl.l.npar * sl.l.vh;   // matrices per field (V)
     char *p = (char *)m;
     auto take = [&](size_t n) {
         char *q = p;
         p += al256(n);
         return q;
     };
-    sl.u = (double2 *)take(3 * 2 * vh * 9 * 16);
-    sl.ut = (double2 *)take(2 * vh * 9 * 16);
-    sl.g = (double2 *)take(2 * vh * 9 * 16);
-    sl.u64r = (double2 *)take(3 * 2 * vh * 6 * 16);
-    sl.g64r = (double2 *)take(2 * vh * 6 * 16);
-    sl.u32 = (float4 *)take(3 * 2 * vh * 3 * 16);
-    sl.g32 = (float4 *)take(2 * vh * 3 * 16);
-    sl.nbx = (int)(((sl.l.vs >> 1) + BCHUNK - 1) / BCHUNK);
+    sl.u = (double2 *)take(3 * mv * 9 * 16);
+    sl.ut = (double2 *)take(mv * 9 * 16);
+    sl.g = (double2 *)take(mv * 9 * 16);
+    sl.u64r = (double2 *)take(3 * mv * 6 * 16);
+    sl.g64r = (double2 *)take(mv * 6 * 16);
+    sl.u32 = (float4 *)take(3 * mv * 3 * 16);
+    sl.g32 = (float4 *)take(mv * 3 * 16);
+    sl.nbx = (int)slot_chunks(sl.l);
     sl.nfull = (int)((sl.l.vs + BCHUNK - 1) / BCHUNK);
     sl.part = (double *)take((size_t)nt * sl.nbx * BPIECES * 2 * 8);
     GFC_CHECK(cudaMemcpyAsync(b->dslots + slot, &sl, sizeof sl, cudaMemcpyHostToDevice, b->s));
@@ -824,6 +951,7 @@ extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
     b->ns[slot] = ns;
     b->nt[slot] = nt;
     b->used_sites += V;
+    b->odd_slots += ns & 1;
     // observables scratch large enough for every slot seen so far
     size_t need = (size_t)nt * obs_blocks_per_slice(sl.l) * 4;
     if (need > b->part_n) {
@@ -861,6 +989,7 @@ extern "C" int gfc_batch_remove(gfc_batch *b, int slot) {
     b->mem[slot] = nullptr;
     b->used[slot] = 0;
     b->used_sites -= (size_t)b->ns[slot] * b->ns[slot] * b->ns[slot] * b->nt[slot];
+    b->odd_slots -= b->ns[slot] & 1;
     b->hs[slot] = BSlot{};
     return GFC_OK;
 }
@@ -919,7 +1048,13 @@ extern "C" int gfc_batch_activate(gfc_batch *b, int slot, int precision) {
     const Lat &l = sl.l;
     launch_identity(sl.g, l, b->s);
     int st;
-    if (precision == GFC_PREC_MIXED) {
+    if (!l.cb) {
+        // odd ns: FP64 on two stored rows in the lexicographic layout, whatever the
+        // precision asked for (the FP32 phase and its switch need the checkerboard)
+        launch_pack2(sl.u, sl.u64r, l.vh, 3 * l.npar, b->s);
+        launch_pack2(sl.g, sl.g64r, l.vh, l.npar, b->s);
+        st = SS_LEX;
+    } else if (precision == GFC_PREC_MIXED) {
         launch_to_f32(sl.u, sl.u32, l.vh, 3 * l.npar, b->s);
         launch_identity32(sl.g32, l.vh, l.npar, b->s);
         st = SS_FP32;
@@ -958,6 +1093,8 @@ static BState make_state(gfc_batch *b, const gfc_params *p, const gfc_options *o
     s.ring = b->ring;
     s.items32 = b->items32;
     s.items64 = b->items64;
+    s.itemslex = b->itemslex;
+    s.lex = b->odd_slots > 0;
     s.pend = b->pend;
     s.cap_items = b->cap_items;
     s.cap_pend = b->cap_pend;
@@ -982,6 +1119,14 @@ static void launch_bsweep_k(int grid, cudaStream_t st, const BState &bs) {
         smem_attr_once(done, kern, bytes);
     }
     kern<<<grid, BCHUNK, bytes, st>>>(bs);
+}
+
+static void launch_bsweep_lex(int grid, cudaStream_t st, const BState &bs, int level) {
+    constexpr size_t bytes = (size_t)6 * S64R::NS * 32 * 16;
+    auto kern = k_bsweep_lex<11>;
+    static std::atomic<unsigned long long> done{0};
+    smem_attr_once(done, kern, bytes);
+    kern<<<grid, 32, bytes, st>>>(bs, level);
 }
 
 template <int MINB>
@@ -1057,6 +1202,11 @@ static void enqueue_round(gfc_batch *b, const BState &bs) {
             launch_bsweep<S32>(b->minb32, false, b->nsm * b->minb32, st, bs);
             launch_bsweep<S64R>(m64, b->stage64 != 0, b->nsm * m64, st, bs);
         }
+        if (bs.lex) {
+            // odd-ns timeslices: the four boundary levels in order, then their e2
+            for (int level = 0; level < 4; level++) launch_bsweep_lex(b->nsm * 11, st, bs, level);
+            k_bmeasure_lex<<<b->nsm * 16, 32, 0, st>>>(bs);
+        }
         k_bslice<<<(b->nslices + 7) / 8, 256, 0, st>>>(bs);
         k_breunit<<<b->grid, BCHUNK, 0, st>>>(bs);
     }
@@ -1095,7 +1245,7 @@ extern "C" int gfc_batch_round(gfc_batch *b, const gfc_params *p, const gfc_opti
     int rc = ensure_graph(b, p, o);
     if (rc) return rc;
     GFC_CHECK(cudaGraphLaunch(b->exec, b->s));
-    b->launches += 4 + (b->minb32 > 4 && b->minb64 > 4 ? 3 : 4) * b->round_k;
+    b->launches += 4 + ((b->minb32 > 4 && b->minb64 > 4 ? 3 : 4) + (b->odd_slots > 0 ? 5 : 0)) * b->round_k;
     b->rounds++;
     GFC_CHECK(cudaMemcpyAsync(b->hcounts, b->counts, sizeof(int) * 8, cudaMemcpyDeviceToHost, b->s));
     GFC_CHECK(cudaMemcpyAsync(b->hstate, b->state, sizeof(int) * b->nslices, cudaMemcpyDeviceToHost, b->s));
@@ -1376,13 +1526,17 @@ extern "C" int gfc_batch_autotune(gfc_batch *b, int ns, int nt, double *times) {
         // FP32 sweep
         if ((rc = gfc_batch_activate(b, slot, GFC_PREC_MIXED))) break;
         double best = 1e30;
-        const int m32[6] = {2, 3, 4, 8, 11, 12}, i32[6] = {0, 1, 2, 11, 12, 13};
+        // one-warp shapes first: they share one launch with the FP64 items
+        // (k_bsweep_wf, whose shape is the FP64 one, so they are timed in that shape),
+        // which saves a launch and a tail per half-sweep when both precisions are
+        // active, something a lattice in FP32 alone does not show; a 128-thread shape
+        // is kept only if it is more than 2 % faster
+        const int m32[6] = {8, 11, 12, 2, 3, 4}, i32[6] = {11, 12, 13, 0, 1, 2};
         for (int q = 0; q < 6 && !rc; q++) {
-            // one-warp FP32 CTAs run in the launch they share with the FP64 items
-            // (k_bsweep_wf), whose shape is the FP64 one: time them in that shape
             gfc_batch_set_shape(b, m32[q], m32[q] > 4 ? m32[q] : (save64 > 4 ? 3 : save64), 4);
             rc = time_rounds(GFC_PREC_MIXED, t[i32[q]]);
-            if (!rc && t[i32[q]] < best) best = t[i32[q]], best32 = m32[q];
+            const double margin = m32[q] > 4 ? 1.0 : 0.98;
+            if (!rc && t[i32[q]] < best * margin) best = t[i32[q]], best32 = m32[q];
         }
         if (rc) break;
         // FP64 sweep

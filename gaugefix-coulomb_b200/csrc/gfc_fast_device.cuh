@@ -542,14 +542,16 @@ __device__ __forceinline__ void apply_backward(typename S::V *__restrict__ p, si
 }
 
 // The e2 density of a site from its current links, without updating anything (the
-// "pre" of fast_site on its own).
-template <class S>
+// "pre" of fast_site on its own).  CB = false: the lexicographic layout of odd ns
+// (one parity slot, i = the site's lexicographic index).
+template <class S, bool CB = true>
 __device__ __forceinline__ double measure_site(const typename S::V *__restrict__ u, const Lat &l, int par,
                                                uint32_t i) {
     using T = typename S::T;
     using C = typename CT<T>::t;
-    const int op = par ^ 1;
-    Coord c = coord_cb(l, par, i);
+    if (!CB) par = 0;
+    const int op = CB ? par ^ 1 : 0;
+    Coord c = CB ? coord_cb(l, par, i) : coord_lex(l, i);
     Mt<T> w;
 #pragma unroll
     for (int k = 0; k < 9; k++) w.e[k] = mkc<C>(T(0), T(0));
@@ -557,7 +559,7 @@ __device__ __forceinline__ double measure_site(const typename S::V *__restrict__
     for (int d = 0; d < 3; d++) {
         Mt<T> f, r;
         S::load(u + su_idx<S>(l, d, par, i), l.vh, f);
-        S::load(u + su_idx<S>(l, d, op, back_L(l, c, d) >> 1), l.vh, r);
+        S::load(u + su_idx<S>(l, d, op, CB ? back_L(l, c, d) >> 1 : back_L(l, c, d)), l.vh, r);
 #pragma unroll
         for (int x = 0; x < 3; x++)
 #pragma unroll
@@ -727,8 +729,9 @@ __device__ __forceinline__ void apply_staged(const typename S::V *src, int sst, 
 // instead of from L2 (the links of the other directions are loaded from global
 // memory twice, as in fast_site).  Staged layout per CTA: entry e of matrix m of
 // thread x at sm[(m * NS + e) * BLOCK + x] (m = 2d forward, 2d+1 backward link of
-// direction d, m = NST for G).  Two-row storage only.
-template <class S, int BLOCK, bool SG, int NST = 6>
+// direction d, m = NST for G).  Two-row storage only.  CB = false: the lexicographic
+// layout of odd ns (one parity slot, i = the site's lexicographic index).
+template <class S, int BLOCK, bool SG, int NST = 6, bool CB = true>
 __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, typename S::V *__restrict__ g,
                                                  const Lat &l, int par, uint32_t i, typename S::T omega,
                                                  unsigned hits, int track, double &pre, double &post,
@@ -737,11 +740,12 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
     using C = typename CT<T>::t;
     using V = typename S::V;
     static_assert(S::ROWS01_ONLY, "staging is for two-row storage");
-    const int op = par ^ 1;
-    Coord c = coord_cb(l, par, i);
+    if (!CB) par = 0;
+    const int op = CB ? par ^ 1 : 0;
+    Coord c = CB ? coord_cb(l, par, i) : coord_lex(l, i);
     uint32_t ib[3];
 #pragma unroll
-    for (int d = 0; d < 3; d++) ib[d] = back_L(l, c, d) >> 1;
+    for (int d = 0; d < 3; d++) ib[d] = CB ? back_L(l, c, d) >> 1 : back_L(l, c, d);
     static_assert(NST == 2 || NST == 4 || NST == 6, "whole directions are staged");
     constexpr int ND = NST / 2;   // staged directions
     V *my = sm + threadIdx.x;

@@ -247,7 +247,7 @@ extern "C" size_t gfc_server_capacity_sites(const gfc_server *s) { return s ? s-
 // copied now and uploaded at admission.
 extern "C" int gfc_server_submit(gfc_server *s, int ns, int nt, const void *links, int elem_bytes, int byteswap,
                                  uint64_t seed, double scale, int precision, int64_t *id) {
-    if (!s || !id || ns <= 0 || nt <= 0 || (ns & 1)) return GFC_ERR_ARG;
+    if (!s || !id || ns <= 0 || nt <= 0) return GFC_ERR_ARG;
     if (links && elem_bytes != 8 && elem_bytes != 4) return GFC_ERR_ARG;
     const size_t V = (size_t)ns * ns * ns * nt;
     if (V > s->max_sites) {

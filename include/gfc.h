@@ -258,11 +258,14 @@ int  gfc_ctx_get_blocking(const gfc_ctx *c, int *slices64, int *sweeps64, int *s
 int  gfc_e2_theta_device_noalloc(int ns, int nt, const double *u_dev, void *stream, double *e2, double *theta);
 
 /* ---- batches: many lattices, per-timeslice retirement (no counterpart in the reference) ---- */
-/* A batch holds up to max_slots lattices (even ns, nt <= max_nt, max_sites sites in
- * total) on one GPU.  Every timeslice of every lattice is swept independently
- * (timeslices share no link during the sweeps) and retires when its own e2 falls
- * below the tolerance (measured on the links it keeps); with GFC_PREC_MIXED it first runs FP32 bulk sweeps until its
- * e2 falls below options.switch_e2 and is then rebuilt in FP64.  One round = K
+/* A batch holds up to max_slots lattices (nt <= max_nt, max_sites sites in total) on
+ * one GPU.  Every timeslice of every lattice is swept independently (timeslices
+ * share no link during the sweeps) and retires when its own e2 falls below the
+ * tolerance (measured on the links it keeps); with GFC_PREC_MIXED it first runs FP32
+ * bulk sweeps until its e2 falls below options.switch_e2 and is then rebuilt in
+ * FP64.  Lattices of odd ns run in FP64 whatever the precision asked for, each
+ * half-sweep in four launches over the boundary levels that keep the reference's
+ * sequential order where same-parity sites share a link.  One round = K
  * half-sweeps of all active timeslices, replayed as a captured CUDA graph.  Slots
  * can be added, activated, finalised and removed between rounds (continuous
  * batching).  Slot memory is allocated stream-ordered (no device synchronisation). */

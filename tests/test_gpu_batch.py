@@ -132,7 +132,7 @@ def test_same_result_alone_and_in_the_mix(shape):
 def test_batch_admission_limits():
     with gfc.Batch(max_sites=5000, max_slots=2, max_nt=8) as b:
         with pytest.raises(gfc.GFCError):
-            b.add(5, 4)                  # odd ns
+            b.add(0, 4)                  # empty lattice
         with pytest.raises(gfc.GFCError):
             b.add(4, 16)                 # nt above max_nt
         s = b.add(8, 8)                  # 4096 sites
@@ -227,3 +227,48 @@ def test_held_slot_gives_the_same_result():
         assert active == 0
         b.finalize(s)
         assert b.download_gt(s).tobytes() == G_alone.tobytes()
+
+
+@pytest.mark.parametrize("precision", [gfc.PREC_MIXED, gfc.PREC_FP64_FAST])
+def test_odd_ns_slots(precision):
+    """Lattices of odd ns (3, 5 and 7) beside an even one: each is fixed (e2 below the
+    tolerance, G in SU(3), links G U0 G^dagger, plaquettes unchanged) to the oracle's
+    gauge functional, and an odd-ns lattice gets the same G alone and in the mix.
+    Odd ns runs in FP64 by boundary levels, whatever the precision asked for."""
+    geoms = [(3, 4, 141, 0.5), (5, 4, 142, 0.6), (7, 6, 143, 0.4), (6, 4, 144, 0.5)]
+    U0 = {}
+    with gfc.Batch(max_sites=10 ** 5, max_slots=6, max_nt=8) as b:
+        slots = []
+        for ns, nt, seed, scale in geoms:
+            s = b.add(ns, nt)
+            U = gfc.synth_config(ns, nt, seed, scale)
+            b.upload(s, U, 8, False)
+            orc.reunitarize(U)
+            U0[s] = U
+            slots.append(s)
+        for s in slots:
+            b.activate(s, precision)
+        rounds, reps = b.fix_all(params(), gfc.options(precision=precision))
+        G5_mix = b.download_gt(slots[1])
+        for s, (ns, nt, seed, scale) in zip(slots, geoms):
+            r = reps[s]
+            assert r.status > 0 and r.e2 <= TOL, (ns, nt, r.status, r.e2)
+            G = b.download_gt(s)
+            U = b.download_links(s)
+            assert su3_error(G) < 1e-13
+            U1 = U0[s].copy()
+            orc.apply_gt(U1, G, ns, nt)
+            np.testing.assert_allclose(U1, U, atol=1e-12)
+            for w in (0, 1):
+                assert orc.plaquette(U, ns, nt, w) == pytest.approx(orc.plaquette(U0[s], ns, nt, w), abs=1e-13)
+            # the oracle's gauge functional at its e2 <= tol (reference schedule, deeper)
+            Uo, Go = U0[s].copy(), np.zeros(ns ** 3 * nt * 18)
+            orc.fix(Uo, Go, ns, nt, tol=TOL)
+            assert r.functional == pytest.approx(orc.functional(Uo, ns, nt), rel=1e-10)
+        assert b.status() == 0
+    with gfc.Batch(max_sites=10 ** 5, max_slots=2, max_nt=8) as b:
+        s = b.add(5, 4)
+        b.upload(s, gfc.synth_config(5, 4, 142, 0.6), 8, False)
+        b.activate(s, precision)
+        b.fix_all(params(), gfc.options(precision=precision))
+        assert b.download_gt(s).tobytes() == G5_mix.tobytes()

@@ -104,3 +104,16 @@ def test_larger_requests_admitted_while_others_run():
             assert rep.status > 0 and rep.e2 <= TOL
     for rid, (ns, nt, sd, sc, pr) in zip(ids, reqs):
         assert out[rid].tobytes() == alone(ns, nt, sd, sc, pr).tobytes()
+
+
+def test_odd_ns_request():
+    """A 5^3x4 request beside an 8^3x8 one: fixed in FP64 by boundary levels, the same
+    G as the lattice alone in a batch."""
+    p = gfc.default_params(tolerance=TOL)
+    with gfc.Server(max_sites=10 ** 5, max_slots=4, max_nt=16) as srv:
+        a = srv.submit(5, 4, seed=151, scale=0.5)
+        b_ = srv.submit(8, 8, seed=152, scale=0.5)
+        out = run_until_done(srv, [a, b_], p, gfc.options(precision=gfc.PREC_MIXED))
+        assert srv.poll(a)[3].e2 <= TOL
+    assert out[a].tobytes() == alone(5, 4, 151, 0.5, gfc.PREC_MIXED).tobytes()
+    assert out[b_].tobytes() == alone(8, 8, 152, 0.5, gfc.PREC_MIXED).tobytes()
