@@ -58,14 +58,14 @@ enum : int { MF_NOW = 1, MF_PREV = 2, MF_DENSE = 4 };
 constexpr int MEASURE_PERIOD = 32;
 __host__ __device__ constexpr int measure_at(int c) { return c % MEASURE_PERIOD >= MEASURE_PERIOD - 2; }
 constexpr int BCHUNK = 128;   // sites per work item = threads per CTA of the sweep kernels
-constexpr int BPIECES = BCHUNK / 32;   // 32-site pieces per item: e2 partials are kept per piece
+constexpr int BPIECES = BCHUNK / 32;   // 32-site pieces of an item (one-warp CTAs sweep them in turn)
 
 struct BSlot {          // device-visible descriptor of one resident lattice
     Lat l;
     double2 *u, *ut, *g;   // FP64 full: canonical links and G
     double2 *u64r, *g64r;  // FP64 two-row working copies
     float4 *u32, *g32;     // FP32 two-row working copies
-    double *part;          // [nt][nbx][BPIECES][2] partials of the fused e2 per 32-site piece
+    double *part;          // [nt][nbx][2] chunk partials of the fused e2
     int nbx;               // chunks per timeslice and parity = ceil(vs/2 / BCHUNK)
     int nfull;             // chunks per timeslice over both parities = ceil(vs / BCHUNK)
 };
@@ -261,11 +261,9 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
                 // the item's sum in its first piece's slot, zeros in the others
                 block_pair_sum(pre, post, sh);   // the sums are valid in thread 0
                 if (threadIdx.x == 0) {
-                    double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * BPIECES * 2;
+                    double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
                     pp[0] = pre;
                     pp[1] = post;
-#pragma unroll
-                    for (int k = 2; k < 2 * BPIECES; k++) pp[k] = 0.0;
                 }
             }
         }
@@ -280,9 +278,10 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
 // the slowest of several warps, and the item's e2 partials are summed over its
 // pieces per lane, then across the warp, in a fixed order.  Each thread stages into
 // and reads back from its own shared-memory slots only, so no CTA barrier is needed.
-// One 32-site piece q of a work item, for k_bsweep_w / k_bsweep_wf.
+// One work item of k_bsweep_w / k_bsweep_wf: its BCHUNK sites in pieces of 32, the
+// e2 partials summed per lane over the pieces and then across the warp.
 template <class S>
-__device__ __forceinline__ void bsweep_piece_w(const BState &b, int2 item, int q, unsigned char *stage) {
+__device__ __forceinline__ void bsweep_item_w(const BState &b, int2 item, unsigned char *stage) {
     using T = typename S::T;
     constexpr bool F64 = sizeof(T) == 8;
     const int lane = threadIdx.x;
@@ -299,38 +298,42 @@ __device__ __forceinline__ void bsweep_piece_w(const BState &b, int2 item, int q
     typename S::V *u, *g;
     slot_fields<S>(sl, u, g);
     const uint32_t vsh = l.vs >> 1;
-    const uint32_t off = (uint32_t)chunk * BCHUNK + (uint32_t)q * 32 + lane;
     double pre = 0.0, post = 0.0;
-    if (off < vsh) {
+#pragma unroll 1
+    for (int q = 0; q < BPIECES; q++) {
+        const uint32_t off = (uint32_t)chunk * BCHUNK + (uint32_t)q * 32 + lane;
+        if (off >= vsh) break;
+        double a = 0.0, z = 0.0;
         if (verify)
-            pre = measure_site<S>(u, l, par, (uint32_t)t * vsh + off);
+            a = measure_site<S>(u, l, par, (uint32_t)t * vsh + off);
         else
-            fast_site_staged<S, 32, false>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, track, pre,
-                                           post, (typename S::V *)stage);
+            fast_site_staged<S, 32, false>(u, g, l, par, (uint32_t)t * vsh + off, (T)b.omega, b.hits, track, a, z,
+                                           (typename S::V *)stage);
+        pre += a;
+        post += z;
     }
-    if (track) {   // a piece past the end of the timeslice contributes zeros
+    if (track) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             pre += __shfl_down_sync(0xffffffffu, pre, o);
             post += __shfl_down_sync(0xffffffffu, post, o);
         }
         if (lane == 0) {
-            double *pp = sl.part + (((size_t)t * sl.nbx + chunk) * BPIECES + q) * 2;
+            double *pp = sl.part + ((size_t)t * sl.nbx + chunk) * 2;
             pp[0] = pre;
             pp[1] = post;
         }
     }
 }
 
-// Both precisions in one persistent launch of one-warp CTAs: the FP32 pieces first,
+// Both precisions in one persistent launch of one-warp CTAs: the FP32 items first,
 // then the FP64 ones, from one cursor, so a half-sweep has one tail instead of one
-// per precision and one launch fewer.  The cursor hands out 32-site pieces, not
-// whole items, so the tail of a half-sweep is one piece long.  A thread's staging
-// slots are the same column of the shared array in both precisions' layouts.
+// per precision and one launch fewer.  A thread's staging slots are the same column
+// of the shared array in both precisions' layouts.
 template <int MINB>
 __global__ void __launch_bounds__(32, MINB) k_bsweep_wf(BState b) {
     extern __shared__ __align__(16) unsigned char bstage[];
-    const int n32 = b.counts[0] * BPIECES, n = n32 + b.counts[1] * BPIECES;
+    const int n32 = b.counts[0], n = n32 + b.counts[1];
     int *cursor = b.counts + 6;
     const int lane = threadIdx.x;
     // the previous half-sweep's reunitarisation flags have been consumed
@@ -339,12 +342,13 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_wf(BState b) {
     if (lane == 0) it = atomicAdd(cursor, 1);
     it = __shfl_sync(0xffffffffu, it, 0);
     while (it < n) {
+        // the next item is requested while this one is swept
         int ahead = 0;
         if (lane == 0) ahead = atomicAdd(cursor, 1);
         if (it < n32)
-            bsweep_piece_w<S32>(b, b.items32[it / BPIECES], it % BPIECES, bstage);
+            bsweep_item_w<S32>(b, b.items32[it], bstage);
         else
-            bsweep_piece_w<S64R>(b, b.items64[(it - n32) / BPIECES], (it - n32) % BPIECES, bstage);
+            bsweep_item_w<S64R>(b, b.items64[it - n32], bstage);
         it = __shfl_sync(0xffffffffu, ahead, 0);
     }
 }
@@ -353,7 +357,7 @@ template <class S, int MINB>
 __global__ void __launch_bounds__(32, MINB) k_bsweep_w(BState b) {
     extern __shared__ __align__(16) unsigned char bstage[];
     constexpr bool F64 = sizeof(typename S::T) == 8;
-    const int n = b.counts[F64 ? 1 : 0] * BPIECES;   // 32-site pieces
+    const int n = b.counts[F64 ? 1 : 0];
     const int2 *items = F64 ? b.items64 : b.items32;
     int *cursor = b.counts + (F64 ? 7 : 6);
     const int lane = threadIdx.x;
@@ -363,10 +367,9 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_w(BState b) {
     if (lane == 0) it = atomicAdd(cursor, 1);
     it = __shfl_sync(0xffffffffu, it, 0);
     while (it < n) {
-        // the next piece is requested while this one is swept
         int ahead = 0;
         if (lane == 0) ahead = atomicAdd(cursor, 1);
-        bsweep_piece_w<S>(b, items[it / BPIECES], it % BPIECES, bstage);
+        bsweep_item_w<S>(b, items[it], bstage);
         it = __shfl_sync(0xffffffffu, ahead, 0);
     }
 }
@@ -413,9 +416,9 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_lex(BState b, int level) {
 }
 
 // e2 of the odd-ns timeslices measured on this half-sweep (mflag MF_NOW), over all
-// their sites, on the state the four level launches left: per-piece partials.
+// their sites, on the state the four level launches left: one partial per item.
 __global__ void __launch_bounds__(32) k_bmeasure_lex(BState b) {
-    const int n = b.counts[10] * BPIECES;
+    const int n = b.counts[10];
     int *cursor = b.counts + 15;
     const int lane = threadIdx.x;
     int it = 0;
@@ -424,18 +427,22 @@ __global__ void __launch_bounds__(32) k_bmeasure_lex(BState b) {
     while (it < n) {
         int ahead = 0;
         if (lane == 0) ahead = atomicAdd(cursor, 1);
-        const int2 item = b.itemslex[it / BPIECES];
-        const int gid = item.x, q = it % BPIECES;
+        const int2 item = b.itemslex[it];
+        const int gid = item.x;
         if (*(volatile int *)&b.state[gid] == SS_LEX && (b.mflag[gid] & MF_NOW)) {   // uniform in the CTA
             const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
             const BSlot &sl = b.slots[slot];
             const Lat &l = sl.l;
-            const uint32_t off = (uint32_t)item.y * BCHUNK + (uint32_t)q * 32 + lane;
-            double v = off < l.vs ? measure_site<S64R, false>(sl.u64r, l, 0, (uint32_t)t * l.vs + off) : 0.0;
+            double v = 0.0;
+#pragma unroll 1
+            for (int q = 0; q < BPIECES; q++) {
+                const uint32_t off = (uint32_t)item.y * BCHUNK + (uint32_t)q * 32 + lane;
+                if (off < l.vs) v += measure_site<S64R, false>(sl.u64r, l, 0, (uint32_t)t * l.vs + off);
+            }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
             if (lane == 0) {
-                double *pp = sl.part + (((size_t)t * sl.nbx + item.y) * BPIECES + q) * 2;
+                double *pp = sl.part + ((size_t)t * sl.nbx + item.y) * 2;
                 pp[0] = v;
                 pp[1] = 0.0;
             }
@@ -473,8 +480,8 @@ __global__ void k_bslice(BState b) {
         const BSlot &sl = b.slots[slot];
         double s0 = 0.0, s1 = 0.0;
         if (f & MF_NOW) {
-            const double *pp = sl.part + (size_t)t * sl.nbx * BPIECES * 2;
-            for (int q = lane; q < sl.nbx * BPIECES; q += 32) {
+            const double *pp = sl.part + (size_t)t * sl.nbx * 2;
+            for (int q = lane; q < sl.nbx; q += 32) {
                 s0 += pp[2 * q];
                 s1 += pp[2 * q + 1];
             }
@@ -876,7 +883,7 @@ extern "C" size_t gfc_batch_slot_bytes(int ns, int nt) {
     return al256(3 * m * 9 * 16) + 2 * al256(m * 9 * 16)            // u, ut, g
            + al256(3 * m * 6 * 16) + al256(m * 6 * 16)              // u64r, g64r
            + al256(3 * m * 3 * 16) + al256(m * 3 * 16)              // u32, g32
-           + al256((size_t)nt * nbx * BPIECES * 2 * 8) + 4096;      // piece partials
+           + al256((size_t)nt * nbx * 2 * 8) + 4096;                // chunk partials
 }
 
 extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
@@ -936,7 +943,7 @@ extern "C" int gfc_batch_add(gfc_batch *b, int ns, int nt, int *slot_out) {
     sl.g32 = (float4 *)take(mv * 3 * 16);
     sl.nbx = (int)slot_chunks(sl.l);
     sl.nfull = (int)((sl.l.vs + BCHUNK - 1) / BCHUNK);
-    sl.part = (double *)take((size_t)nt * sl.nbx * BPIECES * 2 * 8);
+    sl.part = (double *)take((size_t)nt * sl.nbx * 2 * 8);
     GFC_CHECK(cudaMemcpyAsync(b->dslots + slot, &sl, sizeof sl, cudaMemcpyHostToDevice, b->s));
     GFC_CHECK(cudaStreamSynchronize(b->s));   // the host copy of sl goes out of scope
     b->hs[slot] = sl;

@@ -213,6 +213,7 @@ int launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double o
             case 4:   // 55.3 KiB per CTA, 4 CTAs per SM
                 launch_exact_staged<64, 4>(l, u, g, par, omega, hits, s, stop);
                 break;
+
             default:
                 k_sweep_exact<128, 1><<<(l.vh + 127) / 128, 128, 0, s>>>(u, g, l, par, omega, hits, stop);
                 break;
