@@ -5,7 +5,9 @@
 //     (gcc -std=c99, which turns FP contraction off): every product and sum is an
 //     explicitly rounded __dmul_rn / __dadd_rn so the compiler can never fuse them,
 //     complex products use the C99 expansion (ac - bd, ad + bc), complex quotients
-//     use Smith's method, and |z| uses the hypot algorithm glibc ships.  Kernels
+//     use Smith's method, and |z| uses the hypot algorithm glibc ships.  Fused
+//     multiply-adds appear only inside correctly rounded divisions (a method whose
+//     result is the IEEE quotient), never in the reference's own arithmetic.  Kernels
 //     built from these functions reproduce the reference's links and gauge
 //     transformation bit for bit.
 //   * "f" (fast) functions are templated on the storage precision and let the
@@ -210,9 +212,38 @@ __device__ __forceinline__ void xprod_dag(const M3 &a, const M3 &b, M3 &c) {
 // same sequence of rounded operations, so the operands are selected instead of
 // branched on: sites of one warp take different cases, and a branch would run the
 // divisions of both for the whole warp.  The results are those of the branches.
+//
+// All eighteen quotients share the denominator, so they are formed from its
+// correctly rounded reciprocal y by Markstein's method (P. Markstein, "Computation
+// of elementary functions on the IBM RISC System/6000 processor", IBM J. Res. Dev.
+// 34 (1990)): q0 = RN(a y) is within two ulps of a/b; with the remainder
+// r = a - b q, exact by fused multiply-add once q is within one ulp, q1 = RN(q0 + r0 y)
+// is within one ulp and q2 = RN(q1 + r1 y) is the correctly rounded a/b, the value
+// of IEEE division.  The argument needs the operands, quotient and remainder clear
+// of underflow and overflow; outside [2^-500, 2^500] the division is done directly.
+// A zero dividend gives q0, a zero of the quotient's sign.
+__device__ __forceinline__ bool xdiv_in_range(double a) {
+    const double x = fabs(a);
+    return x >= 0x1p-500 && x <= 0x1p+500;
+}
+__device__ __forceinline__ double xdiv_by_rcp(double a, double b, double y) {
+    const double q0 = __dmul_rn(a, y);
+    const double r0 = __fma_rn(-b, q0, a);
+    const double q1 = __fma_rn(r0, y, q0);
+    const double r1 = __fma_rn(-b, q1, a);
+    const double q2 = __fma_rn(r1, y, q1);
+    return a == 0.0 ? q0 : q2;
+}
+// a / b for a divisor b shared by several quotients: y = xrcp(b), b_ok =
+// xdiv_in_range(b); equal to xd(a, b) for every a and b
+__device__ __forceinline__ double xdiv_shared(double a, double b, double y, bool b_ok) {
+    if (b_ok && (a == 0.0 || xdiv_in_range(a))) return xdiv_by_rcp(a, b, y);
+    return xd(a, b);
+}
+
 struct SmithDen {
-    double r, den;
-    int c_ge_d, tiny;
+    double r, den, rcp;
+    int c_ge_d, tiny, rcp_ok;
 };
 __device__ __forceinline__ SmithDen smith_prepare(double2 dd) {
     SmithDen s;
@@ -222,6 +253,8 @@ __device__ __forceinline__ SmithDen smith_prepare(double2 dd) {
     s.r = xd(num, dnm);
     s.den = xa(xm(num, s.r), dnm);                                   // d r + c or c r + d
     s.tiny = !(fabs(s.r) > 2.2250738585072014e-308);
+    s.rcp = xrcp(s.den);
+    s.rcp_ok = xdiv_in_range(s.den);
     return s;
 }
 __device__ __forceinline__ double2 smith_div(double2 x, double2 dd, const SmithDen &s) {
@@ -232,7 +265,8 @@ __device__ __forceinline__ double2 smith_div(double2 x, double2 dd, const SmithD
         const double p = s.c_ge_d ? b : a, q = s.c_ge_d ? a : b;
         const double t = xm(q, s.r);
         const double hi = s.c_ge_d ? b : t, lo = s.c_ge_d ? t : a;
-        return make_double2(xd(xa(xm(p, s.r), q), s.den), xd(xs(hi, lo), s.den));
+        return make_double2(xdiv_shared(xa(xm(p, s.r), q), s.den, s.rcp, s.rcp_ok),
+                            xdiv_shared(xs(hi, lo), s.den, s.rcp, s.rcp_ok));
     }
     if (!s.c_ge_d) return make_double2(xd(xa(xm(c, xd(a, d)), b), s.den), xd(xs(xm(c, xd(b, d)), a), s.den));
     return make_double2(xd(xa(a, xm(d, xd(b, c))), s.den), xd(xs(b, xm(d, xd(a, c))), s.den));

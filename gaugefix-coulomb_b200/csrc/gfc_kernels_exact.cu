@@ -89,6 +89,9 @@ __device__ __forceinline__ void site_update_exact_staged(double2 *__restrict__ u
                                                          unsigned hits, double2 *sm) {
     const int op = par ^ 1;
     const uint32_t si = c.L >> 1;
+    // G is read only after the update is known: ask for it in L2 now
+#pragma unroll
+    for (int e = 0; e < 9; e++) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(g + gidx(l, par, e, si)));
     uint32_t ib[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) ib[d] = back_L(l, c, d) >> 1;
@@ -129,10 +132,10 @@ __device__ __forceinline__ void site_update_exact_staged(double2 *__restrict__ u
     xor_update(w, omega, hits, upd);
     asm volatile("" ::: "memory");   // read the links again from shared memory below
 
-    M3 m, t;
-    load_m(g + gidx(l, par, 0, si), l.vh, m);
-    xprod(upd, m, t);
-    store_m(g + gidx(l, par, 0, si), l.vh, t);
+    // G is loaded here and multiplied after the six link updates, which hide its
+    // latency (the products are independent, so their order changes no result)
+    M3 m, t, gm;
+    load_m(g + gidx(l, par, 0, si), l.vh, gm);
 #pragma unroll 1
     for (int d = 0; d < 3; d++) {
         const uint32_t b = d == 0 ? ib[0] : (d == 1 ? ib[1] : ib[2]);
@@ -143,6 +146,8 @@ __device__ __forceinline__ void site_update_exact_staged(double2 *__restrict__ u
         xprod_dag(m, upd, t);
         store_m(u + uidx(l, d, op, 0, b), l.vh, t);
     }
+    xprod(upd, gm, t);
+    store_m(g + gidx(l, par, 0, si), l.vh, t);
 }
 
 template <int BLOCK, int MINB>
@@ -492,4 +497,55 @@ extern "C" int gfc_device_code_version(int device, int *binary_version, int *ptx
     *binary_version = a.binaryVersion;
     *ptx_version = a.ptxVersion;
     return GFC_OK;
+}
+
+// Self-check of xdiv_shared against IEEE division: count pseudo-random (a, b) pairs,
+// significands random or with many trailing zeros or all ones (exact quotients,
+// near-ties, the divisors next below powers of two), exponents mostly within a
+// factor 2^64 of one and otherwise anywhere (zeros, subnormals, infinities, NaNs).
+namespace gfc {
+__device__ __forceinline__ uint64_t div_mix(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+__device__ double div_operand(uint64_t h, uint64_t form) {
+    uint64_t m = h & 0xFFFFFFFFFFFFFULL, e;
+    if (form % 5 == 0) m = 0xFFFFFFFFFFFFFULL;
+    else if (form % 5 == 1) m = (m >> 30) << 30;
+    if ((form >> 3) % 8 == 0) e = (h >> 52) & 0x7FF;          // anywhere
+    else e = 1023 - 64 + ((h >> 52) & 127);
+    return __longlong_as_double((long long)((h & 0x8000000000000000ULL) | (e << 52) | m));
+}
+__global__ void k_check_division(uint64_t seed, long long count, unsigned long long *bad) {
+    unsigned long long nbad = 0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < count;
+         k += (long long)gridDim.x * blockDim.x) {
+        const uint64_t h1 = div_mix(seed + 2 * (uint64_t)k), h2 = div_mix(h1 ^ 0x5851F42D4C957F2DULL);
+        const uint64_t f = div_mix(h2);
+        const double a = div_operand(h1, f), b = div_operand(h2, f >> 8);
+        const double want = xd(a, b), got = xdiv_shared(a, b, xrcp(b), xdiv_in_range(b));
+        nbad += __double_as_longlong(want) != __double_as_longlong(got);
+    }
+    if (nbad) atomicAdd(bad, nbad);
+}
+}  // namespace gfc
+
+extern "C" int gfc_check_division(int device, unsigned long long seed, long long count,
+                                  unsigned long long *mismatches) {
+    if (!mismatches || count < 0) {
+        gfc::set_error("gfc_check_division: null output or negative count");
+        return GFC_ERR_ARG;
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return gfc::cuda_fail(e, "gfc_check_division: cudaSetDevice");
+    unsigned long long *d = nullptr;
+    if ((e = cudaMalloc(&d, sizeof *d)) != cudaSuccess) return gfc::cuda_fail(e, "gfc_check_division: cudaMalloc");
+    if ((e = cudaMemset(d, 0, sizeof *d)) == cudaSuccess) {
+        gfc::k_check_division<<<148 * 8, 256>>>(seed, count, d);
+        if ((e = cudaGetLastError()) == cudaSuccess && (e = cudaDeviceSynchronize()) == cudaSuccess)
+            e = cudaMemcpy(mismatches, d, sizeof *d, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(d);
+    return e == cudaSuccess ? GFC_OK : gfc::cuda_fail(e, "gfc_check_division");
 }

@@ -100,6 +100,7 @@ def _load():
         "gfc_byteswap": (I, [P, S, S]),
         "gfc_last_error": (ctypes.c_char_p, []),
         "gfc_device_code_version": (I, [I, ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "gfc_check_division": (I, [I, ctypes.c_ulonglong, ctypes.c_longlong, ctypes.POINTER(ctypes.c_ulonglong)]),
         "gfc_host_alloc": (P, [S]),
         "gfc_host_free": (None, [P]),
         "gfc_ctx_create": (I, [I, I, I, I, ctypes.POINTER(P)]),
@@ -183,6 +184,14 @@ def device_code_version(device=0):
     b, p = ctypes.c_int(), ctypes.c_int()
     _check(lib.gfc_device_code_version(device, ctypes.byref(b), ctypes.byref(p)), "gfc_device_code_version")
     return b.value, p.value
+
+
+def check_division(count, seed=1, device=0):
+    """Quotients, of `count` pseudo-random pairs, on which the exact path's shared-
+    divisor division differs from IEEE division (0 expected)."""
+    bad = ctypes.c_ulonglong()
+    _check(lib.gfc_check_division(device, seed, count, ctypes.byref(bad)), "gfc_check_division")
+    return bad.value
 
 
 def synth_config(ns, nt, seed, scale):

@@ -156,6 +156,12 @@ const char *gfc_last_error(void);
  * the virtual architecture it was compiled for (100).  No counterpart in the
  * reference (it has no device code). */
 int  gfc_device_code_version(int device, int *binary_version, int *ptx_version);
+/* Self-check of the division the reference-arithmetic path uses where one divisor
+ * serves several quotients (the explicit inverse's complex division, SU3_ops.c:843-900):
+ * compares it bit for bit with IEEE division on `count` pseudo-random operand pairs
+ * from `seed` and stores the number of differing quotients (0 expected).
+ * Synchronous.  No counterpart in the reference. */
+int  gfc_check_division(int device, unsigned long long seed, long long count, unsigned long long *mismatches);
 /* page-locked host memory for fast transfers (cudaMallocHost / cudaFreeHost) */
 void *gfc_host_alloc(size_t bytes);
 void  gfc_host_free(void *p);

@@ -163,3 +163,11 @@ def test_full_size_halfsweeps_bit_for_bit():
     orc.halfsweep(U, G, ns, nt, 1)
     assert orc.sha(Gg) == orc.sha(G)
     assert orc.sha(Ug.reshape(-1, 4, 18)[:, 1:4, :]) == orc.sha(U.reshape(-1, 4, 18)[:, 1:4, :])
+
+
+def test_shared_divisor_division_is_ieee_division():
+    """The explicit inverse divides nine complex cofactors by one denominator and
+    forms those quotients from its correctly rounded reciprocal (Markstein's
+    method); the result must be IEEE division's on every operand pair, including
+    zeros, subnormals, infinities, NaNs and divisors just below powers of two."""
+    assert gfc.check_division(1 << 30, seed=7) == 0
