@@ -157,6 +157,11 @@ __device__ __forceinline__ double xhypot_kernel(double ax, double ay) {
     const bool a = h <= xm(2.0, ay);
     return xs(h, xd(xa(a ? t1a : t1b, a ? t2a : t2b), xm(2.0, h)));
 }
+// extreme exponents, rescaled by powers of two (out of line: never met in a gauge field)
+static __device__ __noinline__ double xhypot_scaled(double ax, double ay) {
+    if (ax > 0x1p+500) return xm(xhypot_kernel(xm(ax, 0x1p-600), xm(ay, 0x1p-600)), 0x1p+600);
+    return xm(xhypot_kernel(xm(ax, 0x1p+600), xm(ay, 0x1p+600)), 0x1p-600);
+}
 __device__ __forceinline__ double xhypot(double x, double y) {
     double ax = fabs(x), ay = fabs(y);
     if (ax < ay) {
@@ -165,8 +170,7 @@ __device__ __forceinline__ double xhypot(double x, double y) {
         ay = t;
     }
     if (ay <= xm(ax, 0x1p-54)) return xa(ax, ay);
-    if (ax > 0x1p+500) return xm(xhypot_kernel(xm(ax, 0x1p-600), xm(ay, 0x1p-600)), 0x1p+600);
-    if (ay < 0x1p-500) return xm(xhypot_kernel(xm(ax, 0x1p+600), xm(ay, 0x1p+600)), 0x1p-600);
+    if (ax > 0x1p+500 || ay < 0x1p-500) return xhypot_scaled(ax, ay);
     return xhypot_kernel(ax, ay);
 }
 
@@ -234,11 +238,15 @@ __device__ __forceinline__ double xdiv_by_rcp(double a, double b, double y) {
     const double q2 = __fma_rn(r1, y, q1);
     return a == 0.0 ? q0 : q2;
 }
+// The plain division out of line: operands outside the range never occur in a
+// gauge field, and one shared copy keeps the kernels' code (and instruction-cache
+// misses) smaller than eighteen inlined ones.
+static __device__ __noinline__ double xd_rare(double a, double b) { return __ddiv_rn(a, b); }
 // a / b for a divisor b shared by several quotients: y = xrcp(b), b_ok =
 // xdiv_in_range(b); equal to xd(a, b) for every a and b
 __device__ __forceinline__ double xdiv_shared(double a, double b, double y, bool b_ok) {
     if (b_ok && (a == 0.0 || xdiv_in_range(a))) return xdiv_by_rcp(a, b, y);
-    return xd(a, b);
+    return xd_rare(a, b);
 }
 
 struct SmithDen {
@@ -257,6 +265,12 @@ __device__ __forceinline__ SmithDen smith_prepare(double2 dd) {
     s.rcp_ok = xdiv_in_range(s.den);
     return s;
 }
+// Smith's form for a ratio below the smallest normal number (never met in a gauge
+// field; out of line to keep the kernels' code small)
+static __device__ __noinline__ double2 smith_div_tiny(double a, double b, double c, double d, double den, int c_ge_d) {
+    if (!c_ge_d) return make_double2(xd(xa(xm(c, xd(a, d)), b), den), xd(xs(xm(c, xd(b, d)), a), den));
+    return make_double2(xd(xa(a, xm(d, xd(b, c))), den), xd(xs(b, xm(d, xd(a, c))), den));
+}
 __device__ __forceinline__ double2 smith_div(double2 x, double2 dd, const SmithDen &s) {
     const double a = x.x, b = x.y, c = dd.x, d = dd.y;
     if (!s.tiny) {
@@ -268,8 +282,7 @@ __device__ __forceinline__ double2 smith_div(double2 x, double2 dd, const SmithD
         return make_double2(xdiv_shared(xa(xm(p, s.r), q), s.den, s.rcp, s.rcp_ok),
                             xdiv_shared(xs(hi, lo), s.den, s.rcp, s.rcp_ok));
     }
-    if (!s.c_ge_d) return make_double2(xd(xa(xm(c, xd(a, d)), b), s.den), xd(xs(xm(c, xd(b, d)), a), s.den));
-    return make_double2(xd(xa(a, xm(d, xd(b, c))), s.den), xd(xs(b, xm(d, xd(a, c))), s.den));
+    return smith_div_tiny(a, b, c, d, s.den, s.c_ge_d);
 }
 
 // determinant3x3 (SU3_ops.c:251-281)
