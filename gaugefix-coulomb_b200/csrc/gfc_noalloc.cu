@@ -19,9 +19,9 @@
 // to start at zero -- each call writes every slot it later reads.
 //
 // The first call on each device looks up the array's device address
-// (cudaGetSymbolAddress) with that device current and caches it; make that first
-// call before any stream capture.  Every call is synchronous: it copies its two
-// sums back to the host and waits for them on `stream` before returning.
+// (cudaGetSymbolAddress) with that device current and caches it.  Every call is
+// synchronous: it copies its two sums back to the host and waits for them on
+// `stream` before returning.
 //
 // The links must be device memory of the current device (or managed memory):
 // cudaPointerGetAttributes, which allocates nothing, is asked first, and pageable

@@ -254,8 +254,8 @@ int  gfc_ctx_get_blocking(const gfc_ctx *c, int *slices64, int *sweeps64, int *s
  * library (GFC_NOALLOC_SCRATCH_DOUBLES doubles per GPU, held until exit); lattices
  * whose partial sums do not fit are rejected with GFC_ERR_ARG and a message in
  * gfc_last_error().  Calls share that array: calls that overlap on the GPU race.
- * The first call on a device looks up the array's address; make it before any
- * stream capture.  stream is a cudaStream_t (NULL: the legacy default stream).
+ * The first call on a device looks up the array's address (cudaGetSymbolAddress).
+ * stream is a cudaStream_t (NULL: the legacy default stream).
  * The call is synchronous: it copies e2 and theta to the host and waits for them.
  * u_dev must be device memory of the current device or managed memory
  * (cudaPointerGetAttributes is asked first); host memory and another GPU's memory
