@@ -325,6 +325,8 @@ class Lattice:
 
     def autotune(self, which=0):
         """Time every compiled launch shape on this lattice; keep the fastest.
+        The links are kept in the save_links() slot (replacing a copy saved there
+        before) and restored from it afterwards.
         Returns seconds per half-sweep: {"exact": [...], "fast64": [...], "fast32": [...]}."""
         t = np.zeros(49)
         _check(lib.gfc_ctx_autotune(self.h, which, t.ctypes.data), "autotune")

@@ -225,9 +225,11 @@ int  gfc_ctx_apply_gt(gfc_ctx *c);
 /* Times every compiled launch shape (threads per block x resident blocks per SM)
  * of the sweep kernels on this lattice and keeps the fastest for later fixes.
  * which: bit 0 exact FP64, bit 1 fast FP64, bit 2 FP32 (0 = all).  The links are
- * saved and restored around the timing (a device copy of all links is kept) and G
- * is reset to the identity.  times (may be NULL) receives seconds per half-sweep:
- * [0..4] exact shapes (3 plain, 2 with the links staged in shared memory), [5..22]
+ * copied into the slot of gfc_ctx_save_links first (replacing any copy saved there
+ * before) and restored from it after the timing, so the context's links are as
+ * before and a later gfc_ctx_restore_links returns them; G is reset to the
+ * identity.  times (may be NULL) receives seconds per half-sweep:
+ * [0..4] exact shapes (2 plain, 3 with the links staged in shared memory), [5..22]
  * fast FP64 shapes (9 plain, then 9 with links staged in shared memory by cp.async),
  * [23..40] FP32 shapes (same order), [41..44] fast FP64 slice-blocked candidates,
  * [45..48] FP32 slice-blocked candidates.  Slice
