@@ -413,7 +413,8 @@ def vs_golden(g, rep, ps, pt, ps0, pt0):
 
 def run_precision_form(a, gfc):
     """48^3x96, H scale 0.7, seed 3, stored FP32 (big endian) and converted on load:
-    mixed FP32 bulk / FP64 refinement (reunitarised every 10 FP64 half-sweeps) beside
+    mixed FP32 bulk / FP64 refinement (reunitarised every 10 FP64 half-sweeps; switch at
+    e2 < 1e-9, and at 1e-11 with the FP32 links rebuilt every 128 half-sweeps) beside
     the FP64 paths on the same input, each reported against the reference's own fix of
     the same file (final e2, gauge functional, plaquettes)."""
     ns, nt, seed, scale = 48, 96, 3, 0.7
@@ -431,7 +432,11 @@ def run_precision_form(a, gfc):
         runs = [("fp64_exact_arith", gfc.options(precision=gfc.PREC_FP64_EXACT, stop_rule=gfc.STOP_EVERY)),
                 ("fp64_full", gfc.options(precision=gfc.PREC_FP64_FULL, stop_rule=gfc.STOP_EVERY)),
                 ("fp64_fast", gfc.options(precision=gfc.PREC_FP64_FAST, stop_rule=gfc.STOP_EVERY)),
-                ("mixed", gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY, refine_reunit=10))]
+                ("mixed", gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY, refine_reunit=10)),
+                # a later switch with the FP32 links rebuilt from the FP64 start every
+                # 128 half-sweeps (options.switch_e2, options.fp32_refresh)
+                ("mixed_refresh", gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY, refine_reunit=10,
+                                              switch_e2=1e-11, fp32_refresh=128))]
         ref = None
         gold = reference_golden("cfg2_48x96_f32in")
         for name, o in runs:
@@ -443,7 +448,7 @@ def run_precision_form(a, gfc):
             d = dict(seconds=rep.seconds_total, sweeps=rc, final_e2=rep.final_residue, functional=rep.functional,
                      plaq_drift=max(abs(ps - ps0), abs(pt - pt0)),
                      vs_reference_golden=vs_golden(gold, rep, ps, pt, ps0, pt0))
-            if name == "mixed":
+            if name.startswith("mixed"):
                 d["sweeps_fp32"] = rep.sweeps_fp32
             if ref is None:
                 ref = rep
@@ -452,6 +457,7 @@ def run_precision_form(a, gfc):
             res[name] = d
         res["mixed_speedup_vs_fp64_fast"] = res["fp64_fast"]["seconds"] / res["mixed"]["seconds"]
         res["mixed_speedup_vs_fp64_full"] = res["fp64_full"]["seconds"] / res["mixed"]["seconds"]
+        res["mixed_refresh_speedup_vs_fp64_fast"] = res["fp64_fast"]["seconds"] / res["mixed_refresh"]["seconds"]
     raw.close()
     return res
 

@@ -266,22 +266,6 @@ __global__ void k_to_f64(const float4 *__restrict__ src, double2 *__restrict__ d
     for (int e = 0; e < 9; e++) q[(size_t)e * stride] = m.e[e];
 }
 
-// G <- G1 . G on FP64 full SoA blocks ([9][stride] per block), projected back onto
-// SU(3): a warm start's G0 composed with the transformation of the FP32 phase
-__global__ void k_left_mul_gt(const double2 *__restrict__ g1, double2 *__restrict__ g, uint32_t stride,
-                              uint32_t nblk) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
-    if (i >= stride || k >= nblk) return;
-    const size_t o = (size_t)k * 9 * stride + i;
-    Mt<double> a, b, c;
-    S64::load(g1 + o, stride, a);
-    S64::load(g + o, stride, b);
-    fprod_left<S64, double>(a, b, c);
-    if (!fproject(c)) fidentity(c);
-#pragma unroll
-    for (int e = 0; e < 9; e++) g[o + (size_t)e * stride] = c.e[e];
-}
-
 // FP64 full SoA ([9][stride] per block) -> FP64 two-row SoA ([6][stride])
 __global__ void k_pack2(const double2 *__restrict__ src, double2 *__restrict__ dst, uint32_t stride, uint32_t nblk) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
@@ -339,6 +323,71 @@ __global__ void k_identity32(float4 *__restrict__ g, uint32_t stride, uint32_t n
     q[0] = make_float4(1.f, 0.f, 0.f, 0.f);
     q[stride] = make_float4(0.f, 0.f, 0.f, 0.f);
     q[2 * (size_t)stride] = make_float4(1.f, 0.f, 0.f, 0.f);
+}
+
+// Rebuilds of the mixed fix (checkerboard layout; one thread per (parity, site)
+// slot, grid.y = parity).
+//
+// G <- Proj(G32 G) in FP64, G32's two rows widened, completed and projected first
+// (as k_to_f64 does): a warm start's G0, or the G accumulated by earlier rebuilds,
+// composed with the transformation of the FP32 phase; with reset32 the FP32 G
+// restarts from the identity (as k_identity32 sets it).
+__global__ void k_compose_gt(float4 *__restrict__ g32, double2 *__restrict__ g, uint32_t stride, int reset32) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+    if (i >= stride) return;
+    float4 *q = g32 + (size_t)k * 3 * stride + i;
+    const float4 a = q[0], b = q[stride], cc = q[2 * (size_t)stride];
+    Mt<double> m1, m0, r;
+    m1.e[0] = make_double2(a.x, a.y);
+    m1.e[1] = make_double2(a.z, a.w);
+    m1.e[2] = make_double2(b.x, b.y);
+    m1.e[3] = make_double2(b.z, b.w);
+    m1.e[4] = make_double2(cc.x, cc.y);
+    m1.e[5] = make_double2(cc.z, cc.w);
+    if (!fproject(m1)) fidentity(m1);
+    const size_t o = (size_t)k * 9 * stride + i;
+    S64::load(g + o, stride, m0);
+    fprod_left<S64, double>(m1, m0, r);
+    if (!fproject(r)) fidentity(r);
+    S64::store(g + o, stride, r);
+    if (reset32) {
+        q[0] = make_float4(1.f, 0.f, 0.f, 0.f);
+        q[stride] = make_float4(0.f, 0.f, 0.f, 0.f);
+        q[2 * (size_t)stride] = make_float4(1.f, 0.f, 0.f, 0.f);
+    }
+}
+
+// rows 0 and 1 of o into two-row storage (FP32: rounded to nearest)
+__device__ __forceinline__ void store_rows01(float4 *__restrict__ p, size_t st, const Mt<double> &o) {
+    p[0] = make_float4((float)o.e[0].x, (float)o.e[0].y, (float)o.e[1].x, (float)o.e[1].y);
+    p[st] = make_float4((float)o.e[2].x, (float)o.e[2].y, (float)o.e[3].x, (float)o.e[3].y);
+    p[2 * st] = make_float4((float)o.e[4].x, (float)o.e[4].y, (float)o.e[5].x, (float)o.e[5].y);
+}
+__device__ __forceinline__ void store_rows01(double2 *__restrict__ p, size_t st, const Mt<double> &o) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) p[(size_t)c * st] = o.e[c];
+}
+
+// Spatial links from the FP64 start: U_d(x) = G(x) U0_d(x) G(x+d)^dagger (FMA
+// arithmetic), written straight into the two-row storage S of the next phase (FP32
+// for a rebuild of the FP32 phase, FP64 at the switch to the refinement).
+template <class S>
+__global__ void __launch_bounds__(128) k_regauge(const double2 *__restrict__ u0, const double2 *__restrict__ g,
+                                                 typename S::V *__restrict__ out, Lat l) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int par = blockIdx.y;
+    if (i >= l.vh) return;
+    const Coord c = coord_cb(l, par, i);
+    Mt<double> gx, gy, uu, t, o;
+    S64::load(g + gidx(l, par, 0, i), l.vh, gx);
+#pragma unroll 1
+    for (int d = 0; d < 3; d++) {
+        S64::load(g + gidx(l, par ^ 1, 0, fwd_L(l, c, d) >> 1), l.vh, gy);
+        S64::load(u0 + uidx(l, d, par, 0, i), l.vh, uu);
+        fprod_left<S64R, double>(gx, uu, t);   // rows 0, 1 of G(x) U0
+        fprod_dag<S64R, double>(t, gy, o);     // rows 0, 1 of that times G(x+d)^dagger
+        store_rows01(out + su_idx<S>(l, d, par, i), l.vh, o);
+    }
 }
 
 // ------------------------------------------------------------------ host --
@@ -766,14 +815,18 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     // start kept the links as uploaded, before G0 was applied, in u0 already)
     if (!o->warm_start)
         GFC_CHECK(cudaMemcpyAsync(c->u0, c->u, 3 * mat * sizeof(double2), cudaMemcpyDeviceToDevice, c->s));
-    const dim3 gu((l.vh + 255) / 256, 3 * l.npar), gg((l.vh + 255) / 256, l.npar);
+    const dim3 gu((l.vh + 255) / 256, 3 * l.npar), gg((l.vh + 255) / 256, l.npar), gs((l.vh + 127) / 128, l.npar);
     const int maxs = (int)p->max_sweeps_to_fix, K = o->fp32_refresh > 0 ? o->fp32_refresh : 0;
     int done = 0, below = -1;
+    bool rebuilt = false;
     k_to_f32<<<gu, 256, 0, c->s>>>(c->u, (float4 *)c->u32, l.vh, 3 * l.npar);
     k_identity32<<<gg, 256, 0, c->s>>>((float4 *)c->g32, l.vh, l.npar);
     c->launches += 2;
-    // FP32 bulk, in pieces of fp32_refresh half-sweeps when refreshing
-    const unsigned reunit32 = std::min<unsigned>(p->sweeps_to_reunitarization, 50u);
+    // FP32 bulk, in pieces of fp32_refresh half-sweeps when refreshing.  Without
+    // refreshing, the FP32 links and G are reunitarised every min(reunit, 50)
+    // half-sweeps; a refresh rebuilds them from the FP64 start and a projected FP64 G,
+    // which takes the reunitarisation's place.
+    const unsigned reunit32 = K ? 0u : std::min<unsigned>(p->sweeps_to_reunitarization, 50u);
     for (;;) {
         const int lim = K ? std::min(maxs, done + K) : maxs;
         int d = done;
@@ -782,43 +835,40 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
         if (rc) return rc;
         done = d;
         if (below >= 0 || !K || done >= maxs) break;
-        // refresh: G = G32 G in FP64 (projected), links G U0 G^dagger in FP64, rounded
-        // to FP32 again; the FP32 G restarts from the identity
-        if ((rc = ensure_2row(c))) return rc;
-        k_to_f64<<<gg, 256, 0, c->s>>>((const float4 *)c->g32, c->u64r, l.vh, l.npar);
-        k_left_mul_gt<<<gg, 256, 0, c->s>>>(c->u64r, c->g, l.vh, l.npar);
-        launch_apply_gt_spatial(c->u, c->u0, c->g, l, c->s);
-        k_to_f32<<<gu, 256, 0, c->s>>>(c->u, (float4 *)c->u32, l.vh, 3 * l.npar);
-        k_identity32<<<gg, 256, 0, c->s>>>((float4 *)c->g32, l.vh, l.npar);
-        c->launches += 5;
+        // refresh: G = G32 G in FP64 (projected) and the FP32 G back to the identity,
+        // then the FP32 links rounded from G U0 G^dagger computed in FP64
+        k_compose_gt<<<gg, 256, 0, c->s>>>((float4 *)c->g32, c->g, l.vh, 1);
+        k_regauge<S32><<<gs, 128, 0, c->s>>>(c->u0, c->g, (float4 *)c->u32, l);
+        c->launches += 2;
+        rebuilt = true;
     }
     r->sweeps_fp32 = done;
     if (below < 0) {
+        // the FP64 links follow G at the last refresh (the state the FP64 fields hold)
+        if (rebuilt) {
+            launch_apply_gt_spatial(c->u, c->u0, c->g, l, c->s);
+            c->launches++;
+        }
         r->sweeps = done;
         GFC_CHECK(cudaEventRecord(c->ev_d, c->s));
         return GFC_FIX_NOT_CONVERGED;
     }
-    // switch: G in FP64 (rebuilt and projected), U = G U0 G^dagger from the FP64 start
+    // switch: G in FP64 (rebuilt and projected), U = G U0 G^dagger from the FP64 start,
+    // both straight into the two-row storage of the refinement
     if ((rc = ensure_2row(c))) return rc;
-    {
-        if (o->warm_start || K) {
-            // G = G1 G0: G1 of the FP32 phase (FP64, in the two-row buffer, which
-            // is free until the refinement) times the starting G0 (a warm start's,
-            // or the one accumulated by the refreshes)
-            k_to_f64<<<gg, 256, 0, c->s>>>((const float4 *)c->g32, c->u64r, l.vh, l.npar);
-            k_left_mul_gt<<<gg, 256, 0, c->s>>>(c->u64r, c->g, l.vh, l.npar);
-            c->launches += 2;
-        } else {
-            k_to_f64<<<gg, 256, 0, c->s>>>((const float4 *)c->g32, c->g, l.vh, l.npar);
-            c->launches++;
-        }
+    if (o->warm_start || K) {
+        // G = G1 G0: G1 of the FP32 phase times the starting G0 (a warm start's, or
+        // the one accumulated by the refreshes)
+        k_compose_gt<<<gg, 256, 0, c->s>>>((float4 *)c->g32, c->g, l.vh, 0);
+    } else {
+        k_to_f64<<<gg, 256, 0, c->s>>>((const float4 *)c->g32, c->g, l.vh, l.npar);
     }
-    launch_apply_gt_spatial(c->u, c->u0, c->g, l, c->s);
-    c->launches++;
+    k_regauge<S64R><<<gs, 128, 0, c->s>>>(c->u0, c->g, c->u64r, l);
+    k_pack2<<<gg, 256, 0, c->s>>>(c->g, c->g64r, l.vh, l.npar);
+    c->launches += 3;
     // FP64 refinement
     unsigned reunit64 = o->refine_reunit ? o->refine_reunit : p->sweeps_to_reunitarization;
     int done64 = 0;
-    pack_2row(c);
     rc = run_until<S64R>(c, c->u64r, c->g64r, done, (int)p->max_sweeps_to_fix, tol_e2, (double)p->omega_OR,
                          p->hits, reunit64, o->dense_check, &done64, &below);
     if (rc) return rc;
