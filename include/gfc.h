@@ -103,7 +103,9 @@ typedef struct {
     int    fp32_refresh;      /* mixed: every n FP32 half-sweeps fold the FP32 G into an
                                  FP64 G and rebuild the FP32 links from it as G U0
                                  G^dagger in FP64, so FP32 rounding does not accumulate
-                                 in the links (0: off)                                */
+                                 in the links; the FP32 fields are then not
+                                 reunitarised between rebuilds (0: off, FP32
+                                 reunitarisation every min(reunit, 50) half-sweeps)   */
 } gfc_options;
 
 void gfc_options_default(gfc_options *o);
