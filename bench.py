@@ -484,7 +484,7 @@ def parse_mix(spec):
     return mix
 
 
-def run_batch(a, gfc, torch, precision, rk=None):
+def run_batch(a, gfc, torch, precision, rk=None, **opt):
     """The 96-config mix (32 each of 16^3x32, 24^3x48, 32^3x64) in one batch: every
     timeslice retires on its own e2.  Under torchrun the configs are dealt to the
     ranks (config k to rank k mod N, one batch per GPU, no exchange); the time is the
@@ -519,7 +519,7 @@ def run_batch(a, gfc, torch, precision, rk=None):
         torch.cuda.synchronize()
         t_setup = time.perf_counter() - t0
         params = gfc.default_params(tolerance=a.tol)
-        opts = gfc.options(precision=precision)
+        opts = gfc.options(precision=precision, **opt)
         l0 = b.kernel_launches
         if rk:
             rk.barrier()
@@ -567,14 +567,14 @@ def serve_requests(n, rate, seed=7):
 SERVE_WORK_SITES = 40 * 1024 * 1024   # smallest-first: sites sweeping together (one 64^3x128 and others)
 
 
-def run_serve(a, gfc, precision, n_req, rate, policy=None):
+def run_serve(a, gfc, precision, n_req, rate, policy=None, **opt):
     """Poisson stream of requests of mixed sizes through the continuous-batching server.
 
     Latency runs from a request's arrival time to the moment its G is in host
     memory (the server copies it there while the next rounds run)."""
     reqs = serve_requests(n_req, rate)
     params = gfc.default_params(tolerance=a.tol)
-    opts = gfc.options(precision=precision)
+    opts = gfc.options(precision=precision, **opt)
     srv = gfc.Server(max_sites=0, mem_fraction=0.85, max_slots=64, max_nt=128)
     try:
         cap = srv.capacity_sites
@@ -740,13 +740,19 @@ def main():
 
     import gfc
 
+    # the mixed path's later switch with the FP32 fields rebuilt from FP64 every 128
+    # half-sweeps (options.switch_e2, options.fp32_refresh)
+    late = dict(switch_e2=1e-11, fp32_refresh=128)
     if not a.no_batch:   # on every rank: the configs are dealt to the GPUs
         r["extras"]["batch_mixed"] = run_batch(a, gfc, torch, gfc.PREC_MIXED, rk)
+        r["extras"]["batch_mixed_refresh"] = dict(run_batch(a, gfc, torch, gfc.PREC_MIXED, rk, **late), **late)
     if rk.world == 1:
         if not a.no_precision_form and not a.no_extras:
             r["extras"]["precision_form"] = run_precision_form(a, gfc)
         if a.serve_requests > 0:
             r["extras"]["serve_mixed"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate)
+            r["extras"]["serve_mixed_refresh"] = dict(
+                run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate, **late), **late)
             r["extras"]["serve_fp64"] = run_serve(a, gfc, gfc.PREC_FP64_FAST, a.serve_requests, a.serve_rate)
             r["extras"]["serve_mixed_shared"] = run_serve(a, gfc, gfc.PREC_MIXED, a.serve_requests, a.serve_rate,
                                                           gfc.SERVE_ALL)

@@ -89,9 +89,11 @@ struct BState {
     int *counts;          // [0] n32 [1] n64 [2] npend [3] active timeslices [4] half-sweep k [5] overflow
                           // [6] [7] item cursors [8] [9] FP32 / FP64 reunitarisation due
                           // [10] nlex [11..14] cursors of the odd-ns levels [15] of the odd-ns e2 pass
+                          // [16] an FP32 rebuild due
     unsigned *status;
     double omega, switch_e2, tol;
     unsigned hits, reunit32, reunit64;
+    unsigned refresh32;   // options.fp32_refresh: rebuild the FP32 fields every n own half-sweeps
 };
 
 // ------------------------------------------------------------------ compaction --
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
     const int2 *items = F64 ? b.items64 : b.items32;
     int *cursor = b.counts + (F64 ? 7 : 6);
     // the previous half-sweep's reunitarisation flags have been consumed
-    if (!F64 && blockIdx.x == 0 && threadIdx.x == 0) b.counts[8] = b.counts[9] = 0;
+    if (!F64 && blockIdx.x == 0 && threadIdx.x == 0) b.counts[8] = b.counts[9] = b.counts[16] = 0;
     // Items come one at a time from a shared cursor, so a CTA held up by a
     // timeslice's final reduction does not hold back a fixed share of the list.
     // Thread 0 asks for item j + 1 while item j is processed and publishes it in
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_wf(BState b) {
     int *cursor = b.counts + 6;
     const int lane = threadIdx.x;
     // the previous half-sweep's reunitarisation flags have been consumed
-    if (blockIdx.x == 0 && lane == 0) b.counts[8] = b.counts[9] = 0;
+    if (blockIdx.x == 0 && lane == 0) b.counts[8] = b.counts[9] = b.counts[16] = 0;
     int c = 0;
     if (lane == 0) c = atomicAdd(cursor, 1);
     c = __shfl_sync(0xffffffffu, c, 0);
@@ -367,7 +369,7 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_w(BState b) {
     int *cursor = b.counts + (F64 ? 7 : 6);
     const int lane = threadIdx.x;
     // the previous half-sweep's reunitarisation flags have been consumed
-    if (!F64 && blockIdx.x == 0 && lane == 0) b.counts[8] = b.counts[9] = 0;
+    if (!F64 && blockIdx.x == 0 && lane == 0) b.counts[8] = b.counts[9] = b.counts[16] = 0;
     int c = 0;
     if (lane == 0) c = atomicAdd(cursor, 1);
     c = __shfl_sync(0xffffffffu, c, 0);
@@ -572,6 +574,13 @@ __global__ void k_bslice(BState b) {
             nf |= MF_PREV;
         }
         if ((nf & MF_DENSE) || measure_at(c + 1)) nf |= MF_NOW;
+        // an FP32 rebuild after this half-sweep: the next measured pair must not
+        // straddle it (its first half would see the links before the rebuild)
+        const bool rebuild = nst == st && st == SS_FP32 && b.refresh32 && (unsigned)(c + 1) % b.refresh32 == 0;
+        if (rebuild) {
+            nf &= ~MF_PREV;
+            b.counts[16] = 1;
+        }
         b.mflag[gid] = nf;
         b.sweeps[gid] = c + 1;
         if (nst != st) {
@@ -640,6 +649,74 @@ __global__ void __launch_bounds__(BCHUNK) k_breunit(BState b) {
     if (b.lex) breunit_part<S64R>(b, b.reunit64, due, ndue, true);
 }
 
+// ------------------------------------------------------ FP32 rebuilds --
+// With options.fp32_refresh = K, an FP32 timeslice whose own half-sweep count reaches
+// a multiple of K is rebuilt from FP64 (as the single-lattice mixed fix does): pass 1
+// G <- Proj(Proj(G32) G) in FP64 and G32 back to the identity, pass 2 its FP32 links
+// rounded from G(x) U0_d(x) G(x+d)^dagger computed in FP64 from the original links.
+// Both passes return at once unless a rebuild is due this half-sweep; a CTA scans
+// BCHUNK FP32 items at once and rebuilds the chunks of due timeslices only.
+template <int PASS>
+__global__ void __launch_bounds__(BCHUNK) k_brefresh(BState b) {
+    __shared__ int due[BCHUNK];
+    __shared__ int ndue;
+    if (!b.refresh32 || !b.counts[16]) return;   // uniform
+    const int n = b.counts[0];
+    for (int base = blockIdx.x * BCHUNK; base < n; base += gridDim.x * BCHUNK) {
+        if (threadIdx.x == 0) ndue = 0;
+        __syncthreads();
+        const int it = base + threadIdx.x;
+        if (it < n) {
+            const int gid = b.items32[it].x;
+            const int own = b.sweeps[gid];
+            if (b.state[gid] == SS_FP32 && own != 0 && (unsigned)own % b.refresh32 == 0)
+                due[atomicAdd(&ndue, 1)] = it;
+        }
+        __syncthreads();
+        for (int q = 0; q < ndue; q++) {   // independent chunks
+            const int2 item = b.items32[due[q]];
+            const int gid = item.x;
+            const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
+            const BSlot &sl = b.slots[slot];
+            const Lat l = sl.l;
+            const uint32_t span = l.vs >> 1;   // FP32 timeslices use the checkerboard layout
+            const uint32_t off = (uint32_t)item.y * BCHUNK + threadIdx.x;
+            if (off >= span) continue;
+            const uint32_t i = (uint32_t)t * span + off;
+            for (int par = 0; par < 2; par++) {
+                if (PASS == 0) {
+                    float4 *q32 = sl.g32 + sg_idx<S32>(l, par, i);
+                    Mt<float> m32;
+                    S32::load_rows01(q32, l.vh, m32);
+                    Mt<double> m1, m0, r;
+                    for (int e = 0; e < 6; e++) m1.e[e] = make_double2(m32.e[e].x, m32.e[e].y);
+                    if (!fproject(m1)) fidentity(m1);
+                    S64::load(sl.g + sg_idx<S64>(l, par, i), l.vh, m0);
+                    fprod_left<S64, double>(m1, m0, r);
+                    if (!fproject(r)) fidentity(r);
+                    S64::store(sl.g + sg_idx<S64>(l, par, i), l.vh, r);
+                    fidentity(m32);
+                    S32::store(q32, l.vh, m32);
+                } else {
+                    const Coord c = coord_cb(l, par, i);
+                    Mt<double> gx, gy, uu, tm, o;
+                    S64::load(sl.g + sg_idx<S64>(l, par, i), l.vh, gx);
+                    for (int d = 0; d < 3; d++) {
+                        S64::load(sl.g + sg_idx<S64>(l, par ^ 1, fwd_L(l, c, d) >> 1), l.vh, gy);
+                        S64::load(sl.u + uidx(l, d, par, 0, i), l.vh, uu);
+                        fprod_left<S64R, double>(gx, uu, tm);
+                        fprod_dag<S64R, double>(tm, gy, o);
+                        Mt<float> of;
+                        for (int e = 0; e < 6; e++) of.e[e] = make_float2((float)o.e[e].x, (float)o.e[e].y);
+                        S32::store(sl.u32 + su_idx<S32>(l, d, par, i), l.vh, of);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // --------------------------------------------------- FP32 -> FP64 switch --
 // pass 1: G in FP64 (row 2 rebuilt from the FP32 rows, projected) into g and g64r
 __global__ void __launch_bounds__(BCHUNK) k_switch_g(BState b) {
@@ -657,6 +734,14 @@ __global__ void __launch_bounds__(BCHUNK) k_switch_g(BState b) {
         Mt<double> m;
         for (int q = 0; q < 6; q++) m.e[q] = make_double2(m32.e[q].x, m32.e[q].y);
         if (!fproject(m)) fidentity(m);
+        if (b.refresh32) {
+            // composed with the G the rebuilds accumulated
+            Mt<double> m0, r;
+            S64::load(sl.g + sg_idx<S64>(l, s.par, s.i), l.vh, m0);
+            fprod_left<S64, double>(m, m0, r);
+            if (!fproject(r)) fidentity(r);
+            m = r;
+        }
         S64::store(sl.g + sg_idx<S64>(l, s.par, s.i), l.vh, m);
         S64R::store(sl.g64r + sg_idx<S64R>(l, s.par, s.i), l.vh, m);
     }
@@ -812,8 +897,8 @@ extern "C" int gfc_batch_create(int device, size_t max_sites, int max_slots, int
     BTRY(cudaMalloc(&b->items64, sizeof(int2) * b->cap_items));
     BTRY(cudaMalloc(&b->pend, sizeof(int2) * b->cap_pend));
     BTRY(cudaMalloc(&b->itemslex, sizeof(int2) * b->cap_pend));   // chunks over whole timeslices
-    BTRY(cudaMalloc(&b->counts, sizeof(int) * 16));
-    BTRY(cudaMemset(b->counts, 0, sizeof(int) * 16));
+    BTRY(cudaMalloc(&b->counts, sizeof(int) * 17));
+    BTRY(cudaMemset(b->counts, 0, sizeof(int) * 17));
     BTRY(cudaMalloc(&b->status, sizeof(unsigned)));
     BTRY(cudaMemset(b->status, 0, sizeof(unsigned)));
     BTRY(cudaMallocHost(&b->hcounts, sizeof(int) * 8));
@@ -1119,7 +1204,9 @@ static BState make_state(gfc_batch *b, const gfc_params *p, const gfc_options *o
     s.tol = tol;
     s.switch_e2 = std::max(o->switch_e2 > 0 ? o->switch_e2 : 1e-9, tol);
     s.reunit64 = o->refine_reunit ? o->refine_reunit : p->sweeps_to_reunitarization;
-    s.reunit32 = std::min<unsigned>(p->sweeps_to_reunitarization, 50u);
+    s.refresh32 = o->fp32_refresh > 0 ? (unsigned)o->fp32_refresh : 0u;
+    // a rebuild takes the FP32 reunitarisation's place
+    s.reunit32 = s.refresh32 ? 0u : std::min<unsigned>(p->sweeps_to_reunitarization, 50u);
     return s;
 }
 
@@ -1222,6 +1309,10 @@ static void enqueue_round(gfc_batch *b, const BState &bs) {
         }
         k_bslice<<<(b->nslices + 7) / 8, 256, 0, st>>>(bs);
         k_breunit<<<b->grid, BCHUNK, 0, st>>>(bs);
+        if (bs.refresh32) {
+            k_brefresh<0><<<b->grid, BCHUNK, 0, st>>>(bs);
+            k_brefresh<1><<<b->grid, BCHUNK, 0, st>>>(bs);
+        }
     }
 }
 
@@ -1258,7 +1349,8 @@ extern "C" int gfc_batch_round(gfc_batch *b, const gfc_params *p, const gfc_opti
     int rc = ensure_graph(b, p, o);
     if (rc) return rc;
     GFC_CHECK(cudaGraphLaunch(b->exec, b->s));
-    b->launches += 4 + ((b->minb32 > 4 && b->minb64 > 4 ? 3 : 4) + (b->odd_slots > 0 ? 5 : 0)) * b->round_k;
+    b->launches += 4 + ((b->minb32 > 4 && b->minb64 > 4 ? 3 : 4) + (b->odd_slots > 0 ? 5 : 0) +
+                        (o->fp32_refresh > 0 ? 2 : 0)) * b->round_k;
     b->rounds++;
     GFC_CHECK(cudaMemcpyAsync(b->hcounts, b->counts, sizeof(int) * 8, cudaMemcpyDeviceToHost, b->s));
     GFC_CHECK(cudaMemcpyAsync(b->hstate, b->state, sizeof(int) * b->nslices, cudaMemcpyDeviceToHost, b->s));

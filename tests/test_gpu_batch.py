@@ -90,14 +90,52 @@ def test_uneven_batch_fixes_every_lattice(precision, shape):
         assert b.status() == 0
 
 
+@pytest.mark.parametrize("shape", [None, (12, 12)])
+def test_fp32_rebuilds(shape):
+    """options.fp32_refresh in the batch: FP32 timeslices rebuilt from FP64 every 16
+    of their own half-sweeps, a later switch; every lattice still ends in the Coulomb
+    gauge of a single-lattice FP64 fix, with links G U0 G^dagger."""
+    geoms = [(4, 8, 171, 0.4), (6, 6, 172, 0.7), (8, 12, 173, 0.5)]
+    o = gfc.options(precision=gfc.PREC_MIXED, switch_e2=1e-10, fp32_refresh=16)
+    with gfc.Batch(max_sites=10 ** 6, max_slots=8, max_nt=16) as b:
+        if shape:
+            b.set_shape(shape[0], shape[1], 8)
+        U0, slots = {}, []
+        for ns, nt, seed, scale in geoms:
+            s = b.add(ns, nt)
+            U = gfc.synth_config(ns, nt, seed, scale)
+            b.upload(s, U, 8, False)
+            orc.reunitarize(U)
+            U0[s] = U
+            slots.append(s)
+            b.activate(s, gfc.PREC_MIXED)
+        rounds, reps = b.fix_all(params(), o)
+        for s, (ns, nt, seed, scale) in zip(slots, geoms):
+            r = reps[s]
+            assert r.status > 0 and r.e2 <= TOL
+            G, U = b.download_gt(s), b.download_links(s)
+            assert su3_error(G) < 1e-13
+            U1 = U0[s].copy()
+            orc.apply_gt(U1, G, ns, nt)
+            np.testing.assert_allclose(U1, U, atol=1e-12)
+            with gfc.Lattice(ns, nt) as lat:
+                lat.upload_links(U0[s], 8, False)
+                rc, rep1 = lat.fix(params(), gfc.options(precision=gfc.PREC_FP64_FAST, stop_rule=gfc.STOP_EVERY))
+            assert r.functional == pytest.approx(rep1.functional, rel=1e-10)
+            assert b.slice_sweeps(s).max() > 16   # rebuilds ran
+        assert b.status() == 0
+
+
 @pytest.mark.parametrize("shape", SHAPES)
-def test_same_result_alone_and_in_the_mix(shape):
+@pytest.mark.parametrize("refresh", [0, 16])
+def test_same_result_alone_and_in_the_mix(shape, refresh):
     """Continuous batching: a lattice admitted while others are running gets exactly
-    the result it gets alone."""
+    the result it gets alone (also with FP32 rebuilds every 16 own half-sweeps)."""
     ns, nt = 6, 8
     U = gfc.synth_config(ns, nt, 91, 0.5)
     other = gfc.synth_config(8, 8, 92, 0.6)
-    p, o = params(), gfc.options(precision=gfc.PREC_MIXED)
+    p = params()
+    o = gfc.options(precision=gfc.PREC_MIXED, **({"switch_e2": 1e-10, "fp32_refresh": refresh} if refresh else {}))
     with gfc.Batch(max_sites=10 ** 6, max_slots=4, max_nt=16) as b:
         if shape:
             b.set_shape(shape[0], shape[1], 8)
