@@ -324,6 +324,14 @@ def run_extras(a, lat, params, stream, torch, gfc, half):
         g_bit_identical_to_reference=(None if gold is None else
                                       hashlib.sha256(lat.download_gt().tobytes()).hexdigest() == gold["gt_sha256"]),
         reference_half_sweeps=None if gold is None else gold["sweeps"])
+    # fast FP64 on the reference's check schedule (time to tolerance in both stopping
+    # modes): the same half-sweep count as the reference, G to 1e-10 of its G
+    lat.restore_links()
+    rc, repr_s = lat.fix(params, gfc.options(precision=gfc.PREC_FP64_FAST, stop_rule=gfc.STOP_REFERENCE))
+    res["fp64_fast_reference_schedule"] = dict(
+        seconds=repr_s.seconds_total, sweeps=rc, final_e2=repr_s.final_residue,
+        site_updates_per_s=repr_s.sweeps * half / repr_s.seconds_sweeps,
+        reference_half_sweeps=None if gold is None else gold["sweeps"])
     # fast FP64, every-sweep stop (the headline path), for the same-run comparison
     lat.restore_links()
     ps0, pt0 = lat.plaquette()
@@ -652,8 +660,9 @@ def oracle_synth_config(ns, nt, seed, scale):
     return U
 
 
-def cpu_reference(a, steps, warmup, half_sweeps):
-    """The reference's own half-sweep loop (OpenMP over timeslices) on this host."""
+def cpu_reference(a, steps, warmup, half_sweeps, threads=0):
+    """The reference's own half-sweep loop (OpenMP over timeslices) on this host, on
+    `threads` threads (0: all)."""
     exe = ref_harness()
     if exe is None or not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
         return None
@@ -663,7 +672,7 @@ def cpu_reference(a, steps, warmup, half_sweeps):
         cfg = os.path.join(d, "cfg.be")
         U0.astype(">f8").tofile(cfg)
         del U0
-        out = subprocess.run([exe, "bench", cfg, str(ns), str(nt), str(half_sweeps), "0", str(steps),
+        out = subprocess.run([exe, "bench", cfg, str(ns), str(nt), str(half_sweeps), str(threads), str(steps),
                               str(warmup)], capture_output=True, text=True, check=True).stdout
     rows = [ln.split() for ln in out.splitlines() if ln.startswith("step")]
     upd = sum(float(r[3]) for r in rows)
@@ -809,6 +818,9 @@ def main():
                                     "kind": "reference",
                                     "sample": f"{a.cpu_half_sweeps} half-sweeps of {a.ns}^3x{a.nt} "
                                               f"({c['exe']}, reference OR loop, OpenMP over t)"}
+            c1 = cpu_reference(a, 1, 0, 2, threads=1)
+            line["cpu_baseline"]["one_thread"] = {"value": c1["value"], "unit": "site-updates/s", "cores": 1,
+                                                  "sample": f"2 half-sweeps of {a.ns}^3x{a.nt}"}
     if rk.rank == 0:
         print(json.dumps(line))
     rk.close()
