@@ -60,6 +60,8 @@ struct SweepArgs {
     double tol_sum;     // stop when post(sweep-1) + pre(sweep) <= tol_sum
     int test;           // 1: hist holds post(sweep-1) of this run, so the stop test applies
     unsigned *status;
+    int proj;           // 1: project the links written onto SU(3) (reunitarisation folded in;
+                        // honoured by the fully staged two-row FP64 shapes, see links_fold_reunit)
 };
 
 // Launch shapes compiled into the library: (threads per block, minimum resident
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_fast(typename S::V *__res
     if (a.track) fused_reduce<BLOCK>(a, pre, post, sh, last);
 }
 
-template <class S, int BLOCK, int MINB, bool SG, int NST>
+template <class S, int BLOCK, int MINB, bool SG, int NST, bool PROJ = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_staged(typename S::V *__restrict__ u,
                                                               typename S::V *__restrict__ g, SweepArgs a) {
     extern __shared__ __align__(16) unsigned char staged_smem[];
@@ -205,8 +207,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_staged(typename S::V *__r
     const uint32_t off = blockIdx.x * BLOCK + threadIdx.x;
     double pre = 0.0, post = 0.0;
     if (off < vsh)
-        fast_site_staged<S, BLOCK, SG, NST>(u, g, l, a.par, (a.t0 + blockIdx.y) * vsh + off, (T)a.omega, a.hits, a.track,
-                                       pre, post, (typename S::V *)staged_smem);
+        fast_site_staged<S, BLOCK, SG, NST, true, PROJ>(u, g, l, a.par, (a.t0 + blockIdx.y) * vsh + off, (T)a.omega,
+                                                        a.hits, a.track, pre, post, (typename S::V *)staged_smem,
+                                                        a.status);
     if (a.track) {
         // the reduction's scratch reuses the staging buffer: it has no static shared
         // memory, so 32-site blocks fit 12 to an SM; every thread is done with its
@@ -449,7 +452,28 @@ static void launch_staged(dim3 grid, cudaStream_t st, typename S::V *u, typename
     static std::atomic<unsigned long long> done{0};
     smem_attr_once(done, kern, bytes);
     grid.x = ((a.l.vs >> 1) + sh.block - 1) / sh.block;
+    if constexpr (std::is_same<S, S64R>::value && sh.nst == 6) {
+        if (a.proj) {
+            auto kp = k_sweep_staged<S, sh.block, sh.minb, (bool)sh.sg, sh.nst, true>;
+            static std::atomic<unsigned long long> done_p{0};
+            smem_attr_once(done_p, kp, bytes);
+            kp<<<grid, sh.block, bytes, st>>>(u, g, a);
+            return;
+        }
+    }
     kern<<<grid, sh.block, bytes, st>>>(u, g, a);
+}
+
+// Whether a half-sweep launched with SweepArgs::proj projects the links it writes
+// (the fully staged two-row FP64 shapes); the others leave the links to a separate
+// reunitarisation pass.
+template <class S>
+static bool links_fold_reunit(const gfc_ctx *c) {
+    if constexpr (std::is_same<S, S64R>::value) {
+        const int k = c->shape_fast64 - kNumShapes;
+        return k >= 0 && k < kNumStaged && kStaged[k].nst == 6;
+    }
+    return false;
 }
 
 template <class S>
@@ -487,7 +511,8 @@ static void dispatch_fast(int v, dim3 grid, cudaStream_t st, typename S::V *u, t
 // One half-sweep of timeslices [t0, t0 + nsl) (all slices by default).
 template <class S>
 static void launch_fast(gfc_ctx *c, typename S::V *u, typename S::V *g, int sweep, double omega, unsigned hits,
-                        int track, unsigned *stop, double tol_sum, int t0 = 0, int nsl = -1, int test = 1) {
+                        int track, unsigned *stop, double tol_sum, int t0 = 0, int nsl = -1, int test = 1,
+                        int proj = 0) {
     const Lat &l = c->lat;
     TrackPtrs tp = track_ptrs(c);
     SweepArgs a{};
@@ -509,6 +534,7 @@ static void launch_fast(gfc_ctx *c, typename S::V *u, typename S::V *g, int swee
     a.tol_sum = tol_sum;
     a.test = test;
     a.status = c->dstatus;
+    a.proj = proj;
     const int v = sizeof(typename S::T) == 8 ? c->shape_fast64 : c->shape_fast32;
     dispatch_fast<S>(v, dim3(0, nsl < 0 ? l.nt : nsl), c->s, u, g, a);
     c->launches++;
@@ -659,10 +685,15 @@ static int run_until(gfc_ctx *c, typename S::V *u, typename S::V *g, int sweep0,
             const int first_tracked = dense ? sweep : std::max(sweep, end - 2);
             for (; sweep < end; sweep++) {
                 const int tr = sweep >= first_tracked;
-                launch_fast<S>(c, u, g, sweep, omega, hits, tr, tp.stop, tol_sum, 0, -1, tr && prev_tracked);
+                // a reunitarisation due after this half-sweep: the links it writes
+                // (every spatial link) are projected by the sweep itself where the
+                // shape can, leaving G's pass alone
+                const bool ru = reunit && !((sweep + 1) % reunit);
+                const bool fold = ru && links_fold_reunit<S>(c);
+                launch_fast<S>(c, u, g, sweep, omega, hits, tr, tp.stop, tol_sum, 0, -1, tr && prev_tracked, fold);
                 prev_tracked = tr;
-                if (reunit && !((sweep + 1) % reunit)) {
-                    launch_reunit<S>(c, u, 3 * l.npar, tp.stop);
+                if (ru) {
+                    if (!fold) launch_reunit<S>(c, u, 3 * l.npar, tp.stop);
                     launch_reunit<S>(c, g, l.npar, tp.stop);
                 }
             }

@@ -6,6 +6,7 @@
 #include <type_traits>
 
 #include "gfc_device.cuh"
+#include "gfc_internal.h"
 
 namespace gfc {
 
@@ -646,14 +647,55 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // up . f (forward link) or r . up^dagger (backward link) from a staged copy `src`
 // (stride sst) to global `dst` (stride st); rows 0 and 1 are stored, row 2 only
-// enters e2.
-template <class S, bool FWD>
+// enters e2.  PROJ: the link is projected onto SU(3) before it is stored (a
+// reunitarisation folded into the half-sweep).  projectSU3 reads rows 0 and 1 only,
+// so the stored rows are those a separate pass would leave; a null row sets the
+// status bit as that pass does.
+template <class S, bool FWD, bool PROJ = false>
 __device__ __forceinline__ void apply_staged(const typename S::V *src, int sst, typename S::V *__restrict__ dst,
-                                             size_t st, const Mt<typename S::T> &up, int track, double (&cc)[8]) {
+                                             size_t st, const Mt<typename S::T> &up, int track, double (&cc)[8],
+                                             unsigned *status = nullptr) {
     using T = typename S::T;
     using C = typename CT<T>::t;
     const double sg = FWD ? 1.0 : -1.0;
-    if constexpr (S::ROWWISE) {
+    if constexpr (S::ROWWISE && PROJ) {
+        C r2[3];
+        if (FWD || track) {
+            C a[3] = {src[0], src[sst], src[2 * sst]};
+            C b[3] = {src[3 * sst], src[4 * sst], src[5 * sst]};
+            fcross_conj(a, b, r2);
+        }
+        Mt<T> o;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (r == 2 && !track) break;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                C v;
+                if (FWD) {
+                    v = fmul(up.e[EL(r, 0)], (C)src[j * sst]);
+                    v = fmac(v, up.e[EL(r, 1)], (C)src[(3 + j) * sst]);
+                    v = fmac(v, up.e[EL(r, 2)], r2[j]);
+                } else {
+                    const C m0 = r < 2 ? (C)src[(3 * r) * sst] : r2[0];
+                    const C m1 = r < 2 ? (C)src[(3 * r + 1) * sst] : r2[1];
+                    const C m2 = r < 2 ? (C)src[(3 * r + 2) * sst] : r2[2];
+                    v = fmul_conj(m0, up.e[EL(j, 0)]);
+                    v = fmac_conj(v, m1, up.e[EL(j, 1)]);
+                    v = fmac_conj(v, m2, up.e[EL(j, 2)]);
+                }
+                o.e[EL(r, j)] = v;
+            }
+            if (track) {
+                if (r == 0) acc_row<0>(cc, o.e[0], o.e[1], o.e[2], sg);
+                if (r == 1) acc_row<1>(cc, o.e[3], o.e[4], o.e[5], sg);
+                if (r == 2) acc_row<2>(cc, o.e[6], o.e[7], o.e[8], sg);
+            }
+        }
+        if (!fproject(o) && status) atomicOr(status, GFC_STATUS_PROJECT_FAIL);
+#pragma unroll
+        for (int e = 0; e < 6; e++) dst[(size_t)e * st] = o.e[e];
+    } else if constexpr (S::ROWWISE) {
         // one output row at a time; operands are read back from shared memory as
         // needed rather than held (row 2 of the link is rebuilt from rows 0 and 1)
         C r2[3];
@@ -714,12 +756,15 @@ __device__ __forceinline__ void apply_staged(const typename S::V *src, int sst, 
                 o.e[EL(r, j)] = v;
             }
         }
-        S::store(dst, st, o);   // rows 0 and 1
         if (track) {
             acc_mat_row<0>(cc, o, sg);
             acc_mat_row<1>(cc, o, sg);
             acc_mat_row<2>(cc, o, sg);
         }
+        if constexpr (PROJ) {
+            if (!fproject(o) && status) atomicOr(status, GFC_STATUS_PROJECT_FAIL);
+        }
+        S::store(dst, st, o);   // rows 0 and 1
     }
 }
 
@@ -731,11 +776,12 @@ __device__ __forceinline__ void apply_staged(const typename S::V *src, int sst, 
 // thread x at sm[(m * NS + e) * BLOCK + x] (m = 2d forward, 2d+1 backward link of
 // direction d, m = NST for G).  Two-row storage only.  CB = false: the lexicographic
 // layout of odd ns (one parity slot, i = the site's lexicographic index).
-template <class S, int BLOCK, bool SG, int NST = 6, bool CB = true>
+// PROJ: the six links written are projected onto SU(3) first (apply_staged).
+template <class S, int BLOCK, bool SG, int NST = 6, bool CB = true, bool PROJ = false>
 __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, typename S::V *__restrict__ g,
                                                  const Lat &l, int par, uint32_t i, typename S::T omega,
                                                  unsigned hits, int track, double &pre, double &post,
-                                                 typename S::V *sm) {
+                                                 typename S::V *sm, unsigned *status = nullptr) {
     using T = typename S::T;
     using C = typename CT<T>::t;
     using V = typename S::V;
@@ -748,6 +794,7 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
     for (int d = 0; d < 3; d++) ib[d] = CB ? back_L(l, c, d) >> 1 : back_L(l, c, d);
     static_assert(NST == 2 || NST == 4 || NST == 6, "whole directions are staged");
     constexpr int ND = NST / 2;   // staged directions
+    static_assert(!PROJ || ND == 3, "links are projected in the fully staged form only");
     V *my = sm + threadIdx.x;
 #pragma unroll
     for (int d = 0; d < ND; d++) {
@@ -813,10 +860,10 @@ __device__ __forceinline__ void fast_site_staged(typename S::V *__restrict__ u, 
 #pragma unroll 1
         for (int d = 0; d < 3; d++) {
             const uint32_t b = d == 0 ? ib[0] : (d == 1 ? ib[1] : ib[2]);
-            apply_staged<S, true>(my + (2 * d) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, par, i), l.vh, up,
-                                  track_links, cc);
-            apply_staged<S, false>(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, op, b), l.vh, up,
-                                   track_links, cc);
+            apply_staged<S, true, PROJ>(my + (2 * d) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, par, i), l.vh,
+                                        up, track_links, cc, status);
+            apply_staged<S, false, PROJ>(my + (2 * d + 1) * S::NS * BLOCK, BLOCK, u + su_idx<S>(l, d, op, b), l.vh,
+                                         up, track_links, cc, status);
         }
     } else
 #pragma unroll
