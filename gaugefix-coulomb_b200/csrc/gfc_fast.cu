@@ -61,7 +61,7 @@ struct SweepArgs {
     int test;           // 1: hist holds post(sweep-1) of this run, so the stop test applies
     unsigned *status;
     int proj;           // 1: project the links written onto SU(3) (reunitarisation folded in;
-                        // honoured by the fully staged two-row FP64 shapes, see links_fold_reunit)
+                        // honoured by the fully staged two-row shapes, see links_fold_reunit)
 };
 
 // Launch shapes compiled into the library: (threads per block, minimum resident
@@ -452,7 +452,7 @@ static void launch_staged(dim3 grid, cudaStream_t st, typename S::V *u, typename
     static std::atomic<unsigned long long> done{0};
     smem_attr_once(done, kern, bytes);
     grid.x = ((a.l.vs >> 1) + sh.block - 1) / sh.block;
-    if constexpr (std::is_same<S, S64R>::value && sh.nst == 6) {
+    if constexpr ((std::is_same<S, S64R>::value || std::is_same<S, S32>::value) && sh.nst == 6) {
         if (a.proj) {
             auto kp = k_sweep_staged<S, sh.block, sh.minb, (bool)sh.sg, sh.nst, true>;
             static std::atomic<unsigned long long> done_p{0};
@@ -465,12 +465,12 @@ static void launch_staged(dim3 grid, cudaStream_t st, typename S::V *u, typename
 }
 
 // Whether a half-sweep launched with SweepArgs::proj projects the links it writes
-// (the fully staged two-row FP64 shapes); the others leave the links to a separate
-// reunitarisation pass.
+// (the fully staged two-row shapes, FP64 and FP32); the others leave the links to a
+// separate reunitarisation pass.
 template <class S>
 static bool links_fold_reunit(const gfc_ctx *c) {
-    if constexpr (std::is_same<S, S64R>::value) {
-        const int k = c->shape_fast64 - kNumShapes;
+    if constexpr (std::is_same<S, S64R>::value || std::is_same<S, S32>::value) {
+        const int k = (std::is_same<S, S64R>::value ? c->shape_fast64 : c->shape_fast32) - kNumShapes;
         return k >= 0 && k < kNumStaged && kStaged[k].nst == 6;
     }
     return false;
