@@ -365,7 +365,11 @@ __device__ __forceinline__ void block_sum(double (&v)[NQ]) {
     __syncthreads();
 }
 
-// grid (nbx, nt): block bx of slice t sums sites of both parities of slice t
+// grid (nbx, nt): block bx of slice t sums sites of both parities of slice t.  The
+// parities alternate from thread to thread (k -> parity k & 1, slot k >> 1): a
+// site's backward links are the other parity's, so they are read by a neighbouring
+// thread or a recent block and come from L2, not a second time from DRAM, as they
+// would if one parity's half of the slice were swept before the other's.
 __global__ void __launch_bounds__(256) k_obs_partials(const double2 *__restrict__ u, Lat l,
                                                       double *__restrict__ part, const unsigned *stop) {
     if (stop && *(volatile const unsigned *)stop) return;
@@ -374,8 +378,8 @@ __global__ void __launch_bounds__(256) k_obs_partials(const double2 *__restrict_
     const uint32_t n = vsh * l.npar;
     double v[2] = {0.0, 0.0};
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        int par = (int)(k / vsh);
-        uint32_t i = t * vsh + (k % vsh);
+        const int par = l.cb ? (int)(k & 1u) : 0;
+        const uint32_t i = t * vsh + (l.cb ? k >> 1 : k);
         double e2, th;
         if (l.cb) {
             Coord c = coord_cb(l, par, i);
