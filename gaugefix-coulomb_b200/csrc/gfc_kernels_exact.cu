@@ -82,19 +82,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep_exact(double2 *__restrict
 // registers held for them), read back from there for the link update instead of
 // being loaded again.  Arithmetic and order are those of site_update_exact.
 // Staged layout: entry e of link m of thread x at sm[(m * 9 + e) * BLOCK + x],
-// m = 2d forward, 2d+1 backward link of direction d.
-template <int BLOCK>
+// m = 2d forward, 2d+1 backward link of direction d.  CB = false: the lexicographic
+// layout of odd ns (one parity slot, slot index = the site's lexicographic index).
+template <int BLOCK, bool CB = true>
 __device__ __forceinline__ void site_update_exact_staged(double2 *__restrict__ u, double2 *__restrict__ g,
                                                          const Lat &l, int par, const Coord &c, double omega,
                                                          unsigned hits, double2 *sm) {
-    const int op = par ^ 1;
-    const uint32_t si = c.L >> 1;
+    if (!CB) par = 0;
+    const int op = CB ? par ^ 1 : 0;
+    const uint32_t si = CB ? c.L >> 1 : c.L;
     // G is read only after the update is known: ask for it in L2 now
 #pragma unroll
     for (int e = 0; e < 9; e++) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(g + gidx(l, par, e, si)));
     uint32_t ib[3];
 #pragma unroll
-    for (int d = 0; d < 3; d++) ib[d] = back_L(l, c, d) >> 1;
+    for (int d = 0; d < 3; d++) ib[d] = CB ? back_L(l, c, d) >> 1 : back_L(l, c, d);
     double2 *my = sm + threadIdx.x;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -183,19 +185,39 @@ static void launch_exact_staged(const Lat &l, double2 *u, double2 *g, int par, d
 // boundary level, 0..3) therefore puts every such pair in consecutive levels, in
 // the reference's order, and no two sites of one level share a link: sweeping
 // level 0, then 1, 2 and 3, each level in parallel, gives every site the links the
-// sequential sweep gives it, bit for bit.  Lexicographic layout, one thread per site.
-__global__ void __launch_bounds__(128) k_sweep_exact_level(double2 *__restrict__ u, double2 *__restrict__ g, Lat l,
-                                                           int sweep, int level, double omega, unsigned hits,
-                                                           const unsigned *stop) {
+// sequential sweep gives it, bit for bit.  Lexicographic layout.
+//
+// The threads of a launch take the sites of the half-sweep's parity only, k -> the
+// k-th such site in lexicographic order: with ns odd, row R (of ns sites along x)
+// has row parity R & 1, so the sites of parity p in a row are x = p ^ (R & 1), +2,
+// ...; a pair of rows holds exactly ns of them, (ns + 1) / 2 in its first row when
+// p = 0, (ns - 1) / 2 when p = 1.  The lanes of a warp are then all of the swept
+// parity (and mostly of the launch's level), and the six links of a site are staged
+// in shared memory as in the even-ns kernel.
+__device__ __forceinline__ bool odd_parity_site(const Lat &l, int p, uint32_t k, uint32_t &L) {
+    const uint32_t ns = (uint32_t)l.ns;
+    const uint32_t a = p ? (ns - 1) >> 1 : (ns + 1) >> 1;   // in the first (even) row of a pair
+    const uint32_t pair = k / ns, rem = k - pair * ns;
+    const uint32_t R = rem < a ? 2 * pair : 2 * pair + 1;
+    const uint32_t j = rem < a ? rem : rem - a;
+    const uint32_t x = 2 * j + ((uint32_t)p ^ (R & 1u));
+    L = x + ns * R;
+    return R < (uint32_t)l.ns * (uint32_t)l.ns * (uint32_t)l.nt;
+}
+constexpr int LEVEL_BLOCK = 32;
+__global__ void __launch_bounds__(LEVEL_BLOCK, 8) k_sweep_exact_level(double2 *__restrict__ u,
+                                                                     double2 *__restrict__ g, Lat l, int sweep,
+                                                                     int level, double omega, unsigned hits,
+                                                                     const unsigned *stop) {
+    extern __shared__ __align__(16) unsigned char level_stage[];
     if (stop && *(volatile const unsigned *)stop) return;
-    const uint32_t L = blockIdx.x * 128 + threadIdx.x;
-    if (L >= l.v) return;
+    uint32_t L;
+    // BLACKRED_SWEEP (gauge_fixing.c:42): parity (x + y + z + t) & 1 = sweep & 1
+    if (!odd_parity_site(l, sweep & 1, blockIdx.x * LEVEL_BLOCK + threadIdx.x, L)) return;
     Coord c = coord_lex(l, L);
-    const int even = !((c.x ^ c.y ^ c.z ^ c.t) & 1u);
-    if (!(even ^ (sweep & 1))) return;   // BLACKRED_SWEEP (gauge_fixing.c:42)
     const uint32_t e = (uint32_t)l.ns - 1;
     if ((int)(c.x == e) + (int)(c.y == e) + (int)(c.z == e) != level) return;
-    site_update_exact<false>(u, g, l, 0, c, omega, hits);
+    site_update_exact_staged<LEVEL_BLOCK, false>(u, g, l, 0, c, omega, hits, (double2 *)level_stage);
 }
 
 int exact_num_shapes() { return 5; }
@@ -224,9 +246,13 @@ int launch_sweep_exact(double2 *u, double2 *g, const Lat &l, int sweep, double o
                 break;
         }
     } else {
-        const unsigned blocks = (l.v + 127) / 128;
+        // the sites of one parity: ceil(V / 2) at most (V odd when nt is)
+        constexpr size_t bytes = (size_t)6 * 9 * LEVEL_BLOCK * sizeof(double2);
+        static std::atomic<unsigned long long> done{0};
+        smem_attr_once(done, k_sweep_exact_level, bytes);
+        const unsigned blocks = (unsigned)((l.v / 2 + 1 + LEVEL_BLOCK - 1) / LEVEL_BLOCK);
         for (int level = 0; level < 4; level++)
-            k_sweep_exact_level<<<blocks, 128, 0, s>>>(u, g, l, sweep, level, omega, hits, stop);
+            k_sweep_exact_level<<<blocks, LEVEL_BLOCK, bytes, s>>>(u, g, l, sweep, level, omega, hits, stop);
         return 4;
     }
     return 1;

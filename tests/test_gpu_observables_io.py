@@ -119,13 +119,15 @@ def test_apply_gt_matches_oracle_bitwise():
     assert orc.sha(Ug) == orc.sha(Uo)
 
 
-@pytest.mark.parametrize("precision,stop", [(gfc.PREC_FP64_EXACT, gfc.STOP_REFERENCE),
-                                            (gfc.PREC_FP64_FAST, gfc.STOP_EVERY),
-                                            (gfc.PREC_MIXED, gfc.STOP_EVERY)])
-def test_warm_start(precision, stop):
+@pytest.mark.parametrize("precision,stop,refresh", [(gfc.PREC_FP64_EXACT, gfc.STOP_REFERENCE, 0),
+                                                    (gfc.PREC_FP64_FAST, gfc.STOP_EVERY, 0),
+                                                    (gfc.PREC_MIXED, gfc.STOP_EVERY, 0),
+                                                    (gfc.PREC_MIXED, gfc.STOP_EVERY, 16)])
+def test_warm_start(precision, stop, refresh):
     """Fixing from a saved transformation G0: the links fixed are G0 U G0^dagger and
     the G returned is the whole transformation (the oracle: applyGaugeTransformationU,
-    then the fix, then the product)."""
+    then the fix, then the product); also with the mixed path's FP32 rebuilds, which
+    compose G0 with each piece of the FP32 phase."""
     ns, nt = 4, 8
     U0 = gfc.synth_config(ns, nt, 133, 0.5)
     orc.reunitarize(U0)
@@ -137,11 +139,14 @@ def test_warm_start(precision, stop):
     with gfc.Lattice(ns, nt, mixed=precision == gfc.PREC_MIXED) as lat:
         lat.upload_links(U0, 8, False)
         lat.upload_gt(G0, 8, False)
+        extra = {"fp32_refresh": refresh, "switch_e2": 1e-10} if refresh else {}
         rc, rep = lat.fix(gfc.default_params(tolerance=1e-15),
-                          gfc.options(precision=precision, stop_rule=stop, warm_start=1))
+                          gfc.options(precision=precision, stop_rule=stop, warm_start=1, **extra))
         G = lat.download_gt()
         U = lat.download_links()
     assert rep.final_residue <= 1e-15
+    if refresh:
+        assert rep.sweeps_fp32 > refresh   # rebuilds ran
     # the fast paths stop at the first half-sweep below the tolerance (the oracle on
     # the reference schedule later), so their G agrees to what e2 ~ 1e-15 pins down;
     # the FP32 phase of the mixed path also drifts along the residual gauge freedom
