@@ -383,9 +383,23 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_w(BState b) {
     }
 }
 
+// The k-th site of parity p of timeslice t in lexicographic order (odd ns): the
+// timeslice's first row has row parity t & 1 (ns^2 is odd) and rows alternate, so a
+// pair of rows holds exactly ns such sites; false past the last one.
+__device__ __forceinline__ bool odd_parity_site_t(const Lat &l, int p, uint32_t t, uint32_t k, uint32_t &off) {
+    const uint32_t ns = (uint32_t)l.ns;
+    const uint32_t a = ((uint32_t)p ^ (t & 1u)) ? (ns - 1) >> 1 : (ns + 1) >> 1;
+    const uint32_t pair = k / ns, rem = k - pair * ns;
+    const uint32_t R = rem < a ? 2 * pair : 2 * pair + 1;
+    const uint32_t j = rem < a ? rem : rem - a;
+    const uint32_t x = 2 * j + ((uint32_t)p ^ ((R + t) & 1u));
+    off = x + ns * R;
+    return R < ns * ns;
+}
+
 // Odd-ns timeslices, boundary level `level` of one half-sweep: one-warp CTAs take
-// 32-site pieces of the odd-ns work items (chunks of a timeslice in lexicographic
-// order); a lane updates its site if it has the half-sweep's parity and the level.
+// 32-site pieces of the odd-ns work items (chunks of the timeslice's sites of the
+// half-sweep's parity, numbered as above); a lane updates its site if it has the level.
 // Sites of one level share no link, and every pair that does share one is in
 // consecutive levels in the sequential sweep's order (see SS_LEX).
 template <int MINB>
@@ -407,13 +421,16 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_lex(BState b, int level) {
             const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
             const BSlot &sl = b.slots[slot];
             const Lat &l = sl.l;
-            const uint32_t off = (uint32_t)item.y * BCHUNK + (uint32_t)(it % BPIECES) * 32 + lane;
-            if (off < l.vs) {
+            // lanes take the sites of the half-sweep's parity only (k-th such site of
+            // the timeslice); the pieces past the last one have nothing to do
+            const uint32_t k = (uint32_t)item.y * BCHUNK + (uint32_t)(it % BPIECES) * 32 + lane;
+            uint32_t off;
+            if (odd_parity_site_t(l, par, (uint32_t)t, k, off)) {
                 const uint32_t L = (uint32_t)t * l.vs + off;
                 const Coord c = coord_lex(l, L);
                 const uint32_t e = (uint32_t)l.ns - 1;
                 const int lev = (int)(c.x == e) + (int)(c.y == e) + (int)(c.z == e);
-                if ((int)((c.x + c.y + c.z + c.t) & 1u) == par && lev == level) {
+                if (lev == level) {
                     double a = 0.0, z = 0.0;
                     fast_site_staged<S64R, 32, false, 6, false>(sl.u64r, sl.g64r, l, 0, L, b.omega, b.hits, 0, a, z,
                                                                  (double2 *)bstage);
