@@ -841,11 +841,10 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     }
     const double tol_e2 = p->gfix_proxy == GFC_PROXY_THETA ? 6.0 * p->tolerance : p->tolerance;
     const double sw = std::max(o->switch_e2 > 0 ? o->switch_e2 : 1e-9, tol_e2);
-    const size_t mat = (size_t)l.npar * l.vh * 9;
-    // keep the FP64 links of the start; they are re-gauged at the switch (a warm
-    // start kept the links as uploaded, before G0 was applied, in u0 already)
-    if (!o->warm_start)
-        GFC_CHECK(cudaMemcpyAsync(c->u0, c->u, 3 * mat * sizeof(double2), cudaMemcpyDeviceToDevice, c->s));
+    // the FP64 links of the start, re-gauged by the rebuilds and at the switch: the
+    // links as uploaded, before G0 was applied, for a warm start (kept in u0); else
+    // the FP64 links themselves, which nothing writes until the switch
+    const double2 *U0 = o->warm_start ? c->u0 : c->u;
     const dim3 gu((l.vh + 255) / 256, 3 * l.npar), gg((l.vh + 255) / 256, l.npar), gs((l.vh + 127) / 128, l.npar);
     const int maxs = (int)p->max_sweeps_to_fix, K = o->fp32_refresh > 0 ? o->fp32_refresh : 0;
     int done = 0, below = -1;
@@ -869,7 +868,7 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
         // refresh: G = G32 G in FP64 (projected) and the FP32 G back to the identity,
         // then the FP32 links rounded from G U0 G^dagger computed in FP64
         k_compose_gt<<<gg, 256, 0, c->s>>>((float4 *)c->g32, c->g, l.vh, 1);
-        k_regauge<S32><<<gs, 128, 0, c->s>>>(c->u0, c->g, (float4 *)c->u32, l);
+        k_regauge<S32><<<gs, 128, 0, c->s>>>(U0, c->g, (float4 *)c->u32, l);
         c->launches += 2;
         rebuilt = true;
     }
@@ -877,7 +876,10 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     if (below < 0) {
         // the FP64 links follow G at the last refresh (the state the FP64 fields hold)
         if (rebuilt) {
-            launch_apply_gt_spatial(c->u, c->u0, c->g, l, c->s);
+            if (o->warm_start)
+                launch_apply_gt_spatial(c->u, c->u0, c->g, l, c->s);
+            else
+                launch_apply_gt(c->u, c->ut, c->g, l, 0, c->s);   // in place, spatial links only
             c->launches++;
         }
         r->sweeps = done;
@@ -894,7 +896,7 @@ int fix_mixed(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report 
     } else {
         k_to_f64<<<gg, 256, 0, c->s>>>((const float4 *)c->g32, c->g, l.vh, l.npar);
     }
-    k_regauge<S64R><<<gs, 128, 0, c->s>>>(c->u0, c->g, c->u64r, l);
+    k_regauge<S64R><<<gs, 128, 0, c->s>>>(U0, c->g, c->u64r, l);
     k_pack2<<<gg, 256, 0, c->s>>>(c->g, c->g64r, l.vh, l.npar);
     c->launches += 3;
     // FP64 refinement

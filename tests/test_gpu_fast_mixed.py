@@ -188,6 +188,33 @@ def test_sparse_e2_measurement_stops_at_the_same_half_sweep(precision):
     assert out[0] == out[1]
 
 
+@pytest.mark.parametrize("warm", [0, 1])
+def test_mixed_refresh_out_of_sweeps_leaves_a_consistent_state(warm):
+    """A mixed fix with FP32 rebuilds that runs out of half-sweeps in the FP32 phase
+    returns GFC_FIX_NOT_CONVERGED with the FP64 fields at the last rebuild: G in SU(3)
+    and the links equal to G U G^dagger of the links it started from."""
+    ns, nt = 6, 8
+    U0 = gfc.synth_config(ns, nt, 61, 0.6)
+    orc.reunitarize(U0)
+    with gfc.Lattice(ns, nt, mixed=True) as lat:
+        lat.upload_links(U0, 8, False)
+        if warm:
+            lat.set_identity_gt()
+        rc, rep = lat.fix(gfc.default_params(tolerance=1e-15, max_sweeps_to_fix=100),
+                          gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY, switch_e2=1e-12,
+                                      fp32_refresh=32, warm_start=warm))
+        G = lat.download_gt()
+        U = lat.download_links()
+    assert rc == gfc.FIX_NOT_CONVERGED
+    assert su3_error(G) < 1e-13
+    ident = np.zeros((9, 2))
+    ident[[0, 4, 8], 0] = 1.0
+    assert np.abs(G.reshape(-1, 9, 2) - ident).max() > 1e-3   # the rebuilds moved G
+    U1 = U0.copy()
+    orc.apply_gt(U1, G, ns, nt)
+    np.testing.assert_allclose(U1, U, atol=1e-12)
+
+
 @pytest.mark.parametrize("refresh,switch", [(64, 1e-11), (128, 1e-11), (16, 1e-10)])
 def test_mixed_with_fp32_refresh(refresh, switch):
     """The mixed path with the FP32 links rebuilt from the FP64 start (as G U0 G^dagger
