@@ -22,6 +22,12 @@
  *   GFC_GT_OUT    = f64 | f32              (CONV_GT_FROM_WORKING_PRECISION)
  *   GFC_SWAP_OUT  = 0 | 1                  (byte swap of the written G)
  *   GFC_DEVICE    = CUDA device ordinal
+ *   GFC_WRITE_CONFIG = 0 | 1               (also write the gauge-fixed configuration to
+ *                                           <config>fixed: the writeConfig call the
+ *                                           reference's main has commented out,
+ *                                           gauge_fix_coulomb.c:185-191; off by default)
+ *   GFC_CFG_OUT   = f64 | f32              (CONV_CFG_FROM_WORKING_PRECISION)
+ *   GFC_CFG_SWAP_OUT = 0 | 1               (NEED_BYTE_SWAP_OUT)
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -103,6 +109,9 @@ int main(int argc, char *argv[]) {
     const int gt_bytes = !strcmp(env_or("GFC_GT_OUT", "f64"), "f32") ? 4 : 8;
     const int swap_out = atoi(env_or("GFC_SWAP_OUT", "0"));
     const int device = atoi(env_or("GFC_DEVICE", "0"));
+    const int write_cfg = atoi(env_or("GFC_WRITE_CONFIG", "0"));
+    const int cfg_out_bytes = !strcmp(env_or("GFC_CFG_OUT", "f64"), "f32") ? 4 : 8;
+    const int cfg_swap_out = atoi(env_or("GFC_CFG_SWAP_OUT", "0"));
 
     if (!geom_ok) {
         fprintf(stderr, "Loading of file %s failed.\n", config_filename);
@@ -193,6 +202,27 @@ int main(int argc, char *argv[]) {
     printf("Sweeps needed to gauge-fix config from file %s: %d. residue: %3.2E \n", config_filename, sweeps,
            rep.final_residue);
     write_sweeps(config_filename, ns, nt, sweeps);
+
+    /* writeConfig (fields_io.c:405-489) of the gauge-fixed links to <config>fixed, where
+       the reference's main has the call commented out (gauge_fix_coulomb.c:185-191) */
+    if (write_cfg) {
+        const size_t out_size = V * 4 * 18 * (size_t)cfg_out_bytes;
+        char *fixed_name = malloc(strlen(config_filename) + 6);
+        void *out = out_size <= cfg_bytes ? buf : malloc(out_size);
+        int crc = fixed_name && out ? GFC_OK : GFC_ERR_ARG;
+        if (crc == GFC_OK) {
+            strcpy(fixed_name, config_filename);
+            strcat(fixed_name, "fixed");
+            crc = gfc_ctx_download_links(ctx, out, cfg_out_bytes, cfg_swap_out);
+        }
+        if (crc == GFC_OK) crc = gfc_write_all(fixed_name, out, out_size);
+        if (crc)
+            fprintf(stderr, "Fixed config writing failed for config %s.\n", config_filename);
+        else
+            printf("U fixed written for config %s.\n", config_filename);
+        if (out && out != buf) free(out);
+        free(fixed_name);
+    }
 
     /* writeGaugeTransf (fields_io.c:493-565) */
     const size_t gt_size = V * 18 * (size_t)gt_bytes;

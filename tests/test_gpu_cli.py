@@ -47,3 +47,31 @@ def test_cli_not_converged_exit(cases, tmp_path):
     assert p.returncode == 1
     assert "could not be gauge-fixed within the maximum number of sweeps" in p.stderr
     assert not (tmp_path / "g.out").exists()
+
+
+def test_cli_writes_the_fixed_config_when_asked(cases, tmp_path):
+    """GFC_WRITE_CONFIG=1: the gauge-fixed configuration (the writeConfig call the
+    reference's main has commented out) goes to <config>fixed, every link (temporal
+    ones included) equal to G(x) U(x) G(x+mu)^dagger of the reunitarised input with
+    the G written beside it; GFC_CFG_OUT=f32 with GFC_CFG_SWAP_OUT=1 writes the same
+    links as big-endian FP32."""
+    c = cases["l4x8"]
+    ns, nt = c["ns"], c["nt"]
+    write_case(c, tmp_path)
+    U0 = gfc.synth_config(ns, nt, c["seed"], c["scale"])
+    orc.reunitarize(U0)
+    out = {}
+    for tag, extra in (("f64", {}), ("f32", {"GFC_CFG_OUT": "f32", "GFC_CFG_SWAP_OUT": "1"})):
+        env = dict(os.environ, GFC_WRITE_CONFIG="1", **extra)
+        p = subprocess.run([CLI, f"{c['name']}.cfg", "g.out", str(ns), str(nt), f"{c['name']}.par"],
+                           capture_output=True, text=True, cwd=tmp_path, env=env, timeout=600)
+        assert p.returncode == 0, p.stderr
+        assert f"U fixed written for config {c['name']}.cfg." in p.stdout
+        raw = (tmp_path / f"{c['name']}.cfgfixed").read_bytes()
+        out[tag] = np.frombuffer(raw, dtype=np.float64 if tag == "f64" else ">f4").astype(np.float64)
+        G = np.fromfile(tmp_path / "g.out", dtype=np.float64)
+    assert out["f64"].size == ns ** 3 * nt * 4 * 18
+    U1 = U0.copy()
+    orc.apply_gt(U1, G, ns, nt)
+    np.testing.assert_allclose(out["f64"], U1, atol=1e-12)
+    np.testing.assert_array_equal(out["f32"], out["f64"].astype(np.float32).astype(np.float64))
