@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(BCHUNK, MINB) k_bsweep(BState b) {
             const int track = verify ? 1 : (b.mflag[gid] & MF_NOW);
             const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
             const BSlot &sl = b.slots[slot];
-            const Lat &l = sl.l;
+            const Lat l = sl.l;   // a local copy: the stores below cannot be taken to change it
             typename S::V *u, *g;
             slot_fields<S>(sl, u, g);
             const uint32_t vsh = l.vs >> 1;
@@ -276,7 +276,9 @@ __device__ __forceinline__ void bsweep_pieces_w(const BState &b, int2 item, int 
     const int track = verify ? 1 : (b.mflag[gid] & MF_NOW);
     const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
     const BSlot &sl = b.slots[slot];
-    const Lat &l = sl.l;
+    // the geometry in registers: through a reference into the slot table the compiler
+    // would read it again after every store of the update (it cannot rule out aliasing)
+    const Lat l = sl.l;
     typename S::V *u, *g;
     slot_fields<S>(sl, u, g);
     const uint32_t vsh = l.vs >> 1;
@@ -420,7 +422,7 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_lex(BState b, int level) {
             const int par = b.sweeps[gid] & 1;
             const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
             const BSlot &sl = b.slots[slot];
-            const Lat &l = sl.l;
+            const Lat l = sl.l;
             // lanes take the sites of the half-sweep's parity only (k-th such site of
             // the timeslice); the pieces past the last one have nothing to do
             const uint32_t k = (uint32_t)item.y * BCHUNK + (uint32_t)(it % BPIECES) * 32 + lane;
