@@ -396,7 +396,9 @@ __device__ __forceinline__ void block_sum(double (&v)[NQ]) {
 // site's backward links are the other parity's, so they are read by a neighbouring
 // thread or a recent block and come from L2, not a second time from DRAM, as they
 // would if one parity's half of the slice were swept before the other's.
-__global__ void __launch_bounds__(256) k_obs_partials(const double2 *__restrict__ u, Lat l,
+// 128-thread blocks: the six links of a site are all requested at once (~170
+// registers), so three blocks (12 warps) fit on an SM where one 256-thread block did
+__global__ void __launch_bounds__(128) k_obs_partials(const double2 *__restrict__ u, Lat l,
                                                       double *__restrict__ part, const unsigned *stop) {
     if (stop && *(volatile const unsigned *)stop) return;
     const uint32_t t = blockIdx.y;
@@ -484,7 +486,7 @@ int obs_blocks_per_slice(const Lat &l) {
 void launch_obs(const double2 *u, const Lat &l, double *part, double *out, double *slice_out, cudaStream_t s,
                 const unsigned *stop) {
     int nbx = obs_blocks_per_slice(l);
-    k_obs_partials<<<dim3(nbx, l.nt), 256, 0, s>>>(u, l, part, stop);
+    k_obs_partials<<<dim3(nbx, l.nt), 128, 0, s>>>(u, l, part, stop);
     k_finalize<<<1, 256, 0, s>>>(part, l.nt, nbx, 2, out, slice_out, stop);
 }
 
