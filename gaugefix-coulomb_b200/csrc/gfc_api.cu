@@ -506,12 +506,15 @@ extern "C" int gfc_ctx_halfsweeps(gfc_ctx *c, int first_sweep, int n, float omeg
     if (!c->has_links) return GFC_ERR_STATE;
     GFC_CHECK(cudaSetDevice(c->dev));
     const double omega = (double)omega_OR;
-    if (precision == GFC_PREC_FP64_EXACT || !c->lat.cb) {
+    // ns = 1 (one link per direction closing on its site) on the reference-arithmetic
+    // kernel whatever the precision: the fast staged forms update that link once
+    if (precision == GFC_PREC_FP64_EXACT || c->lat.ns == 1) {
         for (int k = 0; k < n; k++) {
             c->launches += launch_sweep_exact(c->u, c->g, c->lat, first_sweep + k, omega, hits, c->s, c->shape_exact);
         }
     } else if (n > 0) {
-        int rc = halfsweeps_fast64(c, first_sweep, n, omega, hits);
+        int rc = c->lat.cb ? halfsweeps_fast64(c, first_sweep, n, omega, hits)
+                           : halfsweeps_odd_fast(c, first_sweep, n, omega, hits);
         if (rc) return rc;
     }
     GFC_CHECK(cudaGetLastError());
@@ -584,12 +587,13 @@ static int fix_reference_schedule(gfc_ctx *c, const gfc_params *p, const gfc_opt
         n = std::min(n, (int)p->max_sweeps_to_fix - sweep);
         n = std::min(n, (int)(p->sweeps_to_reunitarization - sweep % p->sweeps_to_reunitarization));
         n = std::max(n, 1);
-        if (o->precision == GFC_PREC_FP64_EXACT || !l.cb) {
+        if (o->precision == GFC_PREC_FP64_EXACT || l.ns == 1) {
             for (int k = 0; k < n; k++) {
                 c->launches += launch_sweep_exact(c->u, c->g, l, sweep + k, omega, p->hits, c->s, c->shape_exact);
             }
         } else {
-            e = halfsweeps_fast64(c, sweep, n, omega, p->hits);
+            // the fast arithmetic; odd ns on the lexicographic layout by boundary levels
+            e = l.cb ? halfsweeps_fast64(c, sweep, n, omega, p->hits) : halfsweeps_odd_fast(c, sweep, n, omega, p->hits);
             if (e) return e;
         }
         sweep += n;
@@ -752,8 +756,10 @@ extern "C" int gfc_ctx_fix(gfc_ctx *c, const gfc_params *p, const gfc_options *o
     int ret;
     if (mixed) {
         ret = fix_mixed(c, p, opt, r);
-    } else if (opt->stop_rule == GFC_STOP_EVERY && (opt->precision == GFC_PREC_FP64_EXACT || !c->lat.cb)) {
+    } else if (opt->stop_rule == GFC_STOP_EVERY && (opt->precision == GFC_PREC_FP64_EXACT || c->lat.ns == 1)) {
         ret = fix_every_sweep_exact(c, p, opt, r);
+    } else if (opt->stop_rule == GFC_STOP_EVERY && !c->lat.cb) {
+        ret = fix_every_sweep_odd_fast(c, p, opt, r);   // odd ns: fast FP64 (no FP32 phase)
     } else if (opt->stop_rule == GFC_STOP_EVERY) {
         ret = fix_every_sweep(c, p, opt, r);
     } else {

@@ -107,6 +107,22 @@ __host__ __device__ __forceinline__ uint32_t back_L(const Lat &l, const Coord &c
     if (d == 1) return c.y ? c.L - ns : c.L + (ns - 1) * ns;
     return c.x ? c.L - 1 : c.L + (ns - 1);
 }
+// The k-th site of parity p = (x + y + z + t) & 1 in lexicographic order, odd ns: row
+// R (of ns sites along x) has row parity R & 1 (ns is odd, so R = y + ns z + ns^2 t has
+// the parity of y + z + t), so the sites of parity p in a row are x = p ^ (R & 1), +2,
+// ...; a pair of rows holds exactly ns of them, (ns + 1) / 2 in its first row when
+// p = 0, (ns - 1) / 2 when p = 1.  False past the last one.
+__device__ __forceinline__ bool odd_parity_site(const Lat &l, int p, uint32_t k, uint32_t &L) {
+    const uint32_t ns = (uint32_t)l.ns;
+    const uint32_t a = p ? (ns - 1) >> 1 : (ns + 1) >> 1;   // in the first (even) row of a pair
+    const uint32_t pair = k / ns, rem = k - pair * ns;
+    const uint32_t R = rem < a ? 2 * pair : 2 * pair + 1;
+    const uint32_t j = rem < a ? rem : rem - a;
+    const uint32_t x = 2 * j + ((uint32_t)p ^ (R & 1u));
+    L = x + ns * R;
+    return R < (uint32_t)l.ns * (uint32_t)l.ns * (uint32_t)l.nt;
+}
+
 __host__ __device__ __forceinline__ uint32_t fwd_L(const Lat &l, const Coord &c, int d) {
     uint32_t ns = l.ns;
     if (d == 0) return c.z + 1 < ns ? c.L + ns * ns : c.L - (ns - 1) * ns * ns;

@@ -600,6 +600,158 @@ static void launch_reunit(gfc_ctx *c, typename S::V *base, uint32_t nblk, unsign
     c->launches++;
 }
 
+static void print_res(int sweep, double res) { printf("Sweeps: %8d.\t residue: %3.2E \n", sweep, res); }
+
+// ----------------------------------------------------------------- odd ns --
+// Odd ns with the fast arithmetic (FP64 on two stored rows, lexicographic layout): a
+// half-sweep is the four boundary-level launches of the exact path (the sequential
+// sweep's order between every pair of sites that share a link, see
+// k_sweep_exact_level), each thread taking a site of the half-sweep's parity
+// (odd_parity_site) and updating it if it has the launch's level.  e2 is measured by
+// a separate pass over the state a half-sweep leaves: a site's post-update w is not
+// final while a later level updates a neighbour.
+constexpr int LEX_BLOCK = 32;
+__global__ void __launch_bounds__(LEX_BLOCK, 11) k_sweep_lex_fast(double2 *__restrict__ u, double2 *__restrict__ g,
+                                                                 Lat l, int sweep, int level, double omega,
+                                                                 unsigned hits, const unsigned *stop) {
+    extern __shared__ __align__(16) unsigned char lex_stage[];
+    if (stop && *(volatile const unsigned *)stop) return;
+    uint32_t L;
+    if (!odd_parity_site(l, sweep & 1, blockIdx.x * LEX_BLOCK + threadIdx.x, L)) return;
+    const Coord c = coord_lex(l, L);
+    const uint32_t e = (uint32_t)l.ns - 1;
+    if ((int)(c.x == e) + (int)(c.y == e) + (int)(c.z == e) != level) return;
+    double pre = 0.0, post = 0.0;
+    fast_site_staged<S64R, LEX_BLOCK, false, 6, false>(u, g, l, 0, L, omega, hits, 0, pre, post,
+                                                       (double2 *)lex_stage);
+}
+
+static void launch_halfsweep_lex_fast(gfc_ctx *c, int sweep, double omega, unsigned hits, const unsigned *stop) {
+    const Lat &l = c->lat;
+    constexpr size_t bytes = (size_t)6 * S64R::NS * LEX_BLOCK * sizeof(double2);
+    static std::atomic<unsigned long long> done{0};
+    smem_attr_once(done, k_sweep_lex_fast, bytes);
+    const unsigned blocks = (unsigned)((l.v / 2 + 1 + LEX_BLOCK - 1) / LEX_BLOCK);
+    for (int level = 0; level < 4; level++)
+        k_sweep_lex_fast<<<blocks, LEX_BLOCK, bytes, c->s>>>(c->u64r, c->g64r, l, sweep, level, omega, hits, stop);
+    c->launches += 4;
+}
+
+// e2 and theta partials (theta = e2 / 6 identically) per timeslice of the two-row
+// lexicographic links: grid (nbx, nt), fixed summation order
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_e2_lex_fast(const double2 *__restrict__ u, Lat l,
+                                                       double *__restrict__ part, const unsigned *stop) {
+    if (stop && *(volatile const unsigned *)stop) return;
+    __shared__ double sh[2][BLOCK / 32];
+    const uint32_t t = blockIdx.y;
+    double v[2] = {0.0, 0.0};
+    for (uint32_t k = blockIdx.x * BLOCK + threadIdx.x; k < l.vs; k += gridDim.x * BLOCK) {
+        const double e2 = measure_site<S64R, false>(u, l, 0, t * l.vs + k);
+        v[0] += e2;
+        v[1] += 0.5 * e2;   // Re Tr(div A div A^dagger) of the site
+    }
+    fblock_sum<BLOCK, 2>(v, sh);
+    if (threadIdx.x == 0) {
+        const size_t o = ((size_t)t * gridDim.x + blockIdx.x) * 2;
+        part[o] = v[0];
+        part[o + 1] = v[1];
+    }
+}
+
+static void launch_e2_lex_fast(gfc_ctx *c, const unsigned *stop) {
+    const Lat &l = c->lat;
+    const int nbx = obs_blocks_per_slice(l);
+    k_e2_lex_fast<128><<<dim3(nbx, l.nt), 128, 0, c->s>>>(c->u64r, l, c->part, stop);
+    launch_finalize2(c->part, l, nbx, c->dres, c->s, stop);
+    c->launches += 2;
+}
+
+// n half-sweeps from `first` on the two stored rows (packed before, unpacked after),
+// for the reference's check schedule
+int halfsweeps_odd_fast(gfc_ctx *c, int first, int n, double omega, unsigned hits) {
+    int rc = ensure_2row(c);
+    if (rc) return rc;
+    pack_2row(c);
+    for (int k = 0; k < n; k++) launch_halfsweep_lex_fast(c, first + k, omega, hits, nullptr);
+    unpack_2row(c);
+    return GFC_OK;
+}
+
+// Stop at the first half-sweep whose proxy is below the tolerance (the schedule of
+// the exact path's every-half-sweep fix: measured at the end of each chunk of 32 while
+// the tolerance is far, after every half-sweep near it; the test on the device).
+int fix_every_sweep_odd_fast(gfc_ctx *c, const gfc_params *p, const gfc_options *o, gfc_report *r) {
+    const Lat &l = c->lat;
+    const double omega = (double)p->omega_OR;
+    double e2 = 0.0, th = 0.0;
+    int rc = gfc_ctx_e2(c, &e2, &th);
+    if (rc) return rc;
+    const int theta = p->gfix_proxy == GFC_PROXY_THETA;
+    const double res0 = theta ? th : e2;
+    r->initial_residue = res0;
+    if (o->verbose) print_res(0, res0);
+    GFC_CHECK(cudaEventRecord(c->ev_b, c->s));
+    if (res0 <= p->tolerance) {
+        GFC_CHECK(cudaEventRecord(c->ev_d, c->s));
+        r->sweeps = 0;
+        r->first_below_tol = 0;
+        return 0;
+    }
+    if ((rc = ensure_2row(c))) return rc;
+    pack_2row(c);
+    unsigned *stop = c->tickets + (l.nt + 1);
+    GFC_CHECK(cudaMemsetAsync(stop, 0, sizeof(unsigned), c->s));
+    const int max = (int)p->max_sweeps_to_fix, period = (int)p->sweeps_to_reunitarization;
+    unsigned hstop = 0;
+    bool dense = o->dense_check != 0;
+    int sweep = 0, k_a = -1;
+    double res_a = 0.0;
+    while (sweep < max) {
+        int end = std::min(max, sweep + 32);
+        if (period > 0) end = std::min(end, (sweep / period + 1) * period);
+        for (; sweep < end; sweep++) {
+            launch_halfsweep_lex_fast(c, sweep, omega, p->hits, stop);
+            if (dense || sweep + 1 == end) {
+                launch_e2_lex_fast(c, stop);
+                launch_exact_check(c->dres, l, theta, p->tolerance, sweep + 1, stop, c->s);
+                c->launches++;
+            }
+        }
+        GFC_CHECK(cudaMemcpyAsync(c->hres + 16, stop, sizeof(unsigned), cudaMemcpyDeviceToHost, c->s));
+        GFC_CHECK(cudaMemcpyAsync(c->hres + 20, c->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        GFC_CHECK(cudaStreamSynchronize(c->s));
+        GFC_CHECK(cudaGetLastError());
+        memcpy(&hstop, c->hres + 16, sizeof hstop);
+        if (hstop) break;
+        if (!dense) {
+            const double res_k = theta ? c->hres[21] / (3.0 * (double)l.v) : c->hres[20] / (double)l.v;
+            if (!(res_k == res_k)) break;   // NaN: reported by the final observables
+            if (res_k <= 1e3 * p->tolerance) {
+                dense = true;
+            } else if (k_a >= 0 && res_k < res_a) {
+                const double rate = pow(res_k / res_a, 1.0 / (double)(sweep - k_a));
+                if (res_k * pow(rate, 64.0) <= 10.0 * p->tolerance) dense = true;
+            }
+            k_a = sweep;
+            res_a = res_k;
+        }
+        if (period > 0 && !(sweep % period)) {
+            launch_reunit<S64R>(c, c->u64r, 3 * l.npar, stop);
+            launch_reunit<S64R>(c, c->g64r, l.npar, stop);
+        }
+    }
+    unpack_2row(c);
+    GFC_CHECK(cudaEventRecord(c->ev_d, c->s));
+    if (hstop) {
+        sweep = (int)hstop;
+        r->first_below_tol = sweep;
+    }
+    r->sweeps = sweep;
+    r->site_updates = (long long)sweep * (l.v / 2);
+    return hstop ? sweep : GFC_FIX_NOT_CONVERGED;
+}
+
 static int ensure_ring(gfc_ctx *c, int ring_n) {
     if (c->ring_n >= ring_n) return GFC_OK;
     cudaFree(c->ring);
@@ -629,7 +781,6 @@ static void sweep_round(gfc_ctx *c, typename S::V *u, typename S::V *g, int swee
     }
 }
 
-static void print_res(int sweep, double res) { printf("Sweeps: %8d.\t residue: %3.2E \n", sweep, res); }
 
 static int initial_proxy(gfc_ctx *c, const gfc_params *p, double *e2, double *res) {
     double th;

@@ -39,6 +39,7 @@ int exact_num_shapes();
 void launch_reunitarize(double2 *base, uint32_t stride, uint32_t nblk, unsigned *status, cudaStream_t s);
 void launch_identity(double2 *g, const Lat &l, cudaStream_t s);
 int obs_blocks_per_slice(const Lat &l);
+void launch_finalize2(const double *part, const Lat &l, int nbx, double *out, cudaStream_t s, const unsigned *stop);
 void launch_obs(const double2 *u, const Lat &l, double *part, double *out, double *slice_out, cudaStream_t s,
                 const unsigned *stop = nullptr);
 // proxy of out (launch_obs) <= tol sets *stop = sweep (once)

@@ -187,23 +187,10 @@ static void launch_exact_staged(const Lat &l, double2 *u, double2 *g, int par, d
 // level 0, then 1, 2 and 3, each level in parallel, gives every site the links the
 // sequential sweep gives it, bit for bit.  Lexicographic layout.
 //
-// The threads of a launch take the sites of the half-sweep's parity only, k -> the
-// k-th such site in lexicographic order: with ns odd, row R (of ns sites along x)
-// has row parity R & 1, so the sites of parity p in a row are x = p ^ (R & 1), +2,
-// ...; a pair of rows holds exactly ns of them, (ns + 1) / 2 in its first row when
-// p = 0, (ns - 1) / 2 when p = 1.  The lanes of a warp are then all of the swept
-// parity (and mostly of the launch's level), and the six links of a site are staged
-// in shared memory as in the even-ns kernel.
-__device__ __forceinline__ bool odd_parity_site(const Lat &l, int p, uint32_t k, uint32_t &L) {
-    const uint32_t ns = (uint32_t)l.ns;
-    const uint32_t a = p ? (ns - 1) >> 1 : (ns + 1) >> 1;   // in the first (even) row of a pair
-    const uint32_t pair = k / ns, rem = k - pair * ns;
-    const uint32_t R = rem < a ? 2 * pair : 2 * pair + 1;
-    const uint32_t j = rem < a ? rem : rem - a;
-    const uint32_t x = 2 * j + ((uint32_t)p ^ (R & 1u));
-    L = x + ns * R;
-    return R < (uint32_t)l.ns * (uint32_t)l.ns * (uint32_t)l.nt;
-}
+// The threads of a launch take the sites of the half-sweep's parity only
+// (odd_parity_site): the lanes of a warp are then all of the swept parity (and
+// mostly of the launch's level), and the six links of a site are staged in shared
+// memory as in the even-ns kernel.
 constexpr int LEVEL_BLOCK = 32;
 __global__ void __launch_bounds__(LEVEL_BLOCK, 8) k_sweep_exact_level(double2 *__restrict__ u,
                                                                      double2 *__restrict__ g, Lat l, int sweep,
@@ -217,7 +204,13 @@ __global__ void __launch_bounds__(LEVEL_BLOCK, 8) k_sweep_exact_level(double2 *_
     Coord c = coord_lex(l, L);
     const uint32_t e = (uint32_t)l.ns - 1;
     if ((int)(c.x == e) + (int)(c.y == e) + (int)(c.z == e) != level) return;
-    site_update_exact_staged<LEVEL_BLOCK, false>(u, g, l, 0, c, omega, hits, (double2 *)level_stage);
+    // ns = 1: a site's forward and backward link in a direction are one link, updated
+    // twice in turn (g U, then that times g^dagger); the unstaged form reads it again
+    // between the two, the staged one would not
+    if (l.ns == 1)
+        site_update_exact<false>(u, g, l, 0, c, omega, hits);
+    else
+        site_update_exact_staged<LEVEL_BLOCK, false>(u, g, l, 0, c, omega, hits, (double2 *)level_stage);
 }
 
 int exact_num_shapes() { return 5; }
@@ -481,6 +474,11 @@ int obs_blocks_per_slice(const Lat &l) {
     if (nb > want) nb = want;
     if (nb < 1) nb = 1;
     return nb;
+}
+
+// sums of nbx per-block (e2, theta) partials per timeslice into out[0..1]
+void launch_finalize2(const double *part, const Lat &l, int nbx, double *out, cudaStream_t s, const unsigned *stop) {
+    k_finalize<<<1, 256, 0, s>>>(part, l.nt, nbx, 2, out, nullptr, stop);
 }
 
 void launch_obs(const double2 *u, const Lat &l, double *part, double *out, double *slice_out, cudaStream_t s,

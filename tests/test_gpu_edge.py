@@ -89,3 +89,31 @@ def test_batch_edge_lattices_alone_and_mixed():
             G = b.download_gt(s)
             assert su3_error(G) < 1e-13
             assert G.tobytes() == alone[g].tobytes()
+
+
+@pytest.mark.parametrize("ns,nt", [(1, 4), (3, 2), (5, 3)])
+@pytest.mark.parametrize("prec", [gfc.PREC_FP64_EXACT, gfc.PREC_FP64_FAST])
+def test_half_sweeps_on_odd_ns(ns, nt, prec):
+    """Half-sweeps on odd ns (the fix of ns = 1 never sweeps: its e2 vanishes
+    identically): the exact path gives the oracle's links and G bit for bit after each
+    half-sweep, ns = 1 included, where a link is its site's forward and backward link
+    and is updated twice in turn; the fast path gives them to rounding."""
+    U = unfixed(ns, nt, 71)
+    V = ns ** 3 * nt
+    Uo, Go = U.copy(), np.zeros(V * 18)
+    Go[0::18] = Go[8::18] = Go[16::18] = 1.0
+    with gfc.Lattice(ns, nt) as lat:
+        lat.upload_links(U, 8, False)
+        lat.set_identity_gt()
+        for k in range(4):
+            lat.halfsweeps(k, 1, 1.95, 2, prec)
+            orc.halfsweep(Uo, Go, ns, nt, k)
+            G = lat.download_gt()
+            Ug = lat.download_links()
+            if prec == gfc.PREC_FP64_EXACT or ns == 1:
+                assert orc.sha(G) == orc.sha(Go), k
+                assert orc.sha(Ug.reshape(-1, 4, 18)[:, 1:4, :]) == orc.sha(Uo.reshape(-1, 4, 18)[:, 1:4, :]), k
+            else:
+                np.testing.assert_allclose(G, Go, atol=1e-13)
+                np.testing.assert_allclose(Ug.reshape(-1, 4, 18)[:, 1:4, :], Uo.reshape(-1, 4, 18)[:, 1:4, :],
+                                           atol=1e-13)
