@@ -418,7 +418,10 @@ __global__ void __launch_bounds__(32, MINB) k_bsweep_lex(BState b, int level) {
         if (lane == 0) ahead = atomicAdd(cursor, 1);
         const int2 item = b.itemslex[it / BPIECES];
         const int gid = item.x;
-        if (*(volatile int *)&b.state[gid] == SS_LEX) {   // uniform in the CTA
+        // ns = 1: every spatial link closes on its own site and e2 vanishes identically,
+        // so the fix leaves the lattice as it is (the half-sweeps pass it by until its
+        // first e2 measurement retires it)
+        if (*(volatile int *)&b.state[gid] == SS_LEX && b.slots[gid / b.max_nt].l.ns > 1) {   // uniform in the CTA
             const int par = b.sweeps[gid] & 1;
             const int slot = gid / b.max_nt, t = gid - slot * b.max_nt;
             const BSlot &sl = b.slots[slot];

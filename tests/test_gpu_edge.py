@@ -65,7 +65,7 @@ def test_fast_paths_on_edge_lattices(ns, nt, prec):
 def test_batch_edge_lattices_alone_and_mixed():
     """Tiny and single-timeslice lattices beside a larger one retire correctly and
     give the same G as when fixed alone."""
-    geoms = [(2, 1, 63), (4, 1, 64), (2, 3, 65), (6, 4, 66)]
+    geoms = [(2, 1, 63), (4, 1, 64), (2, 3, 65), (6, 4, 66), (1, 4, 67)]
     p, o = gfc.default_params(tolerance=TOL), gfc.options(precision=gfc.PREC_MIXED)
     alone = {}
     for ns, nt, seed in geoms:
@@ -89,6 +89,11 @@ def test_batch_edge_lattices_alone_and_mixed():
             G = b.download_gt(s)
             assert su3_error(G) < 1e-13
             assert G.tobytes() == alone[g].tobytes()
+            # the links returned are G U G^dagger of the uploaded ones (ns = 1: unchanged)
+            ns, nt = g
+            U0 = unfixed(ns, nt, dict((k[:2], k[2]) for k in geoms)[g])
+            orc.apply_gt(U0, G, ns, nt)
+            np.testing.assert_allclose(b.download_links(s), U0, atol=1e-12)
 
 
 @pytest.mark.parametrize("ns,nt", [(1, 4), (3, 2), (5, 3)])
