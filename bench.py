@@ -350,43 +350,28 @@ def run_extras(a, lat, params, stream, torch, gfc, half):
     res["fp64_full"] = dict(seconds=repf.seconds_total, sweeps=rc, final_e2=repf.final_residue,
                             functional=repf.functional, plaq_drift=max(abs(psf - ps0), abs(ptf - pt0)),
                             storage="full 3x3", vs_reference_golden=vs_golden(gold, repf, psf, ptf, ps0, pt0))
-    # mixed: FP32 two-row bulk to e2 < 1e-9, FP64 refinement
-    mixed = gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY)
-    lat.restore_links()
-    lat.fix(params, mixed)   # warm
-    best = None
-    for _ in range(2):
+    # mixed: FP32 two-row bulk to e2 < 1e-9, FP64 refinement; the same with a later
+    # switch (e2 < 1e-11) and the FP32 links rebuilt from the FP64 start every 128
+    # half-sweeps (options.fp32_refresh)
+    for name, kw in [("mixed", {}), ("mixed_refresh", dict(switch_e2=1e-11, fp32_refresh=128))]:
+        o = gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY, **kw)
         lat.restore_links()
-        rc, rep = lat.fix(params, mixed)
-        if best is None or rep.seconds_total < best[1].seconds_total:
-            best = (rc, rep)
-    rc, rep = best
-    psm, ptm = lat.plaquette()
-    res["mixed"] = dict(seconds=rep.seconds_total, sweeps=rc, sweeps_fp32=rep.sweeps_fp32,
-                        final_e2=rep.final_residue, functional=rep.functional,
-                        functional_vs_fp64=rep.functional - rep64.functional,
-                        plaq_drift=max(abs(psm - ps0), abs(ptm - pt0)),
-                        vs_reference_golden=vs_golden(gold, rep, psm, ptm, ps0, pt0))
-    res["mixed_speedup_vs_fp64_fast"] = rep64.seconds_total / rep.seconds_total
-    res["mixed_speedup_vs_fp64_full"] = repf.seconds_total / rep.seconds_total
-    # the same with a later switch (e2 < 1e-11) and the FP32 links rebuilt from the
-    # FP64 start every 128 half-sweeps (options.fp32_refresh)
-    late = gfc.options(precision=gfc.PREC_MIXED, stop_rule=gfc.STOP_EVERY, switch_e2=1e-11, fp32_refresh=128)
-    lat.restore_links()
-    lat.fix(params, late)   # warm
-    bestr = None
-    for _ in range(2):
-        lat.restore_links()
-        rcr, repr_ = lat.fix(params, late)
-        if bestr is None or repr_.seconds_total < bestr[1].seconds_total:
-            bestr = (rcr, repr_)
-    rcr, repr_ = bestr
-    psr, ptr = lat.plaquette()
-    res["mixed_refresh"] = dict(seconds=repr_.seconds_total, sweeps=rcr, sweeps_fp32=repr_.sweeps_fp32,
-                                switch_e2=1e-11, fp32_refresh=128, final_e2=repr_.final_residue,
-                                functional=repr_.functional, plaq_drift=max(abs(psr - ps0), abs(ptr - pt0)),
-                                vs_reference_golden=vs_golden(gold, repr_, psr, ptr, ps0, pt0))
-    res["mixed_refresh_speedup_vs_fp64_fast"] = rep64.seconds_total / repr_.seconds_total
+        lat.fix(params, o)   # warm
+        best = None
+        for _ in range(2):
+            lat.restore_links()
+            rcm, repm = lat.fix(params, o)
+            if best is None or repm.seconds_total < best[1].seconds_total:
+                best = (rcm, repm)
+        rcm, repm = best
+        psm, ptm = lat.plaquette()
+        res[name] = dict(seconds=repm.seconds_total, sweeps=rcm, sweeps_fp32=repm.sweeps_fp32,
+                         final_e2=repm.final_residue, functional=repm.functional,
+                         functional_vs_fp64=repm.functional - rep64.functional,
+                         plaq_drift=max(abs(psm - ps0), abs(ptm - pt0)),
+                         vs_reference_golden=vs_golden(gold, repm, psm, ptm, ps0, pt0), **kw)
+        res[name + "_speedup_vs_fp64_fast"] = rep64.seconds_total / repm.seconds_total
+    res["mixed_speedup_vs_fp64_full"] = repf.seconds_total / res["mixed"]["seconds"]
     # isolated kernel timings (no fused reduction, no stopping test)
     lat.restore_links()
     res["kernel_fp64_fast_s"] = timed_halfsweeps(lat, stream, torch, 64, gfc.PREC_FP64_FAST)

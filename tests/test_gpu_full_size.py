@@ -173,25 +173,34 @@ def test_fast_paths_reference_schedule_full_size(raw, precision):
     assert rep.functional == pytest.approx(c["F"], rel=1e-12)
 
 
+FORMS = {
+    "fast": dict(precision=gfc.PREC_FP64_FAST),
+    "full": dict(precision=gfc.PREC_FP64_FULL),
+    "mixed": dict(precision=gfc.PREC_MIXED, refine_reunit=10),
+    # a later switch, the FP32 links rebuilt from the FP64 start every 128 half-sweeps
+    "mixed_refresh": dict(precision=gfc.PREC_MIXED, switch_e2=1e-11, fp32_refresh=128),
+}
+
+
 @pytest.mark.parametrize("name", list(FULL))
-@pytest.mark.parametrize("precision", [gfc.PREC_FP64_FAST, gfc.PREC_FP64_FULL, gfc.PREC_MIXED])
-def test_every_sweep_stop_full_size(raw, name, precision):
+@pytest.mark.parametrize("form", list(FORMS))
+def test_every_sweep_stop_full_size(raw, name, form):
     """Stopping at the first half-sweep with e2 <= 1e-15: the final e2, the gauge
     functional and the plaquettes against the reference's fix of the same input."""
     c = FULL[name]
+    precision = FORMS[form]["precision"]
     with gfc.Lattice(c["ns"], c["nt"], mixed=precision == gfc.PREC_MIXED) as lat:
         load(lat, c, raw)
         ps0, pt0 = lat.plaquette()
         rc, rep = lat.fix(gfc.default_params(tolerance=1e-15),
-                          gfc.options(precision=precision, stop_rule=gfc.STOP_EVERY,
-                                      refine_reunit=10 if precision == gfc.PREC_MIXED else 0))
+                          gfc.options(stop_rule=gfc.STOP_EVERY, **FORMS[form]))
         ps1, pt1 = lat.plaquette()
         e2, _ = lat.e2_theta()
         G = sample(lat.download_gt(), c)
     gold = np.load(os.path.join(GOLDEN, f"{name}_gt_sample.npy"))[1]
     sites = np.arange(0, c["ns"] ** 3 * c["nt"], c["sample_stride"])
     res, drift = global_rotation_residual(G, gold, sites // c["ns"] ** 3)
-    print(f"\n{name} precision {precision}: {rc} half-sweeps, e2 {e2:.3e}, "
+    print(f"\n{name} {form}: {rc} half-sweeps, e2 {e2:.3e}, "
           f"F - F_ref {rep.functional - c['F']:.2e}, plaquette drift {max(abs(ps1 - ps0), abs(pt1 - pt0)):.1e}, "
           f"max |dG| {np.abs(G - gold).max():.1e}, after removing h(t) {res:.1e} (|h(t) - 1| <= {drift:.1e})")
     assert rc > 0 and rep.final_residue <= 1e-15 and e2 <= 1e-15
