@@ -42,11 +42,13 @@ struct gfc_ctx {
     long long launches = 0;
     // launch shapes of the sweep kernels (indices into the compiled shape tables;
     // defaults until gfc_ctx_autotune measures them for this lattice)
-    // (the defaults are the shapes measured fastest at 32^3x64 on a B200: exact with
-    // staged links 128x2, fast FP64 staged in blocks of 32 sites, FP32 plain 128x5)
-    int shape_exact = 3;
-    int shape_fast64 = 13;
-    int shape_fast32 = 7;
+    // (the defaults are the shapes the autotuner picks at 32^3x64 on a B200: exact with
+    // the links staged in blocks of 64 sites, 4 per SM (368-376 us per half-sweep);
+    // fast FP64 and FP32 with links and G staged in blocks of 64 sites, 5 per SM
+    // (215-216 us and 111-112 us; the plain FP32 128 x 5 shape takes 127-129 us))
+    int shape_exact = 4;
+    int shape_fast64 = 10;
+    int shape_fast32 = 10;
     int tuned = 0;
     // slice blocking of the fast sweeps: groups of blk*_slices timeslices run
     // blk*_sweeps half-sweeps each while resident in L2 (0 / 1: not blocked)
